@@ -1,0 +1,416 @@
+#!/usr/bin/env python
+"""Walk-steps/s of GraphWalker's raw-random-walk hot path on one or more B200s.
+
+Workload (one "step"): R-MAT scale 24 (16,777,216 vertices, edge factor 16,
+a/b/c/d = 0.57/0.19/0.19/0.05, self-loops dropped, duplicates kept, ids
+permuted; graph seed 1), CSR split into 32 blocks by the reference's
+compute_block rule and fully resident in HBM; one walk per vertex, fixed
+length 10, uniform neighbour choice, the reference's 0.15 else-branch with
+jump to a uniform vertex (RandomWalkwithJump), Philox stream seed 42, uint32
+visit counts per vertex (the rwdomination sink).  A step clears the counts
+and runs every walk to its end: exactly 16,777,216 x 10 = 167,772,160 walk
+steps.
+
+    python bench.py [--gpus N --steps K --warmup W]            # this engine
+    python bench.py --impl reference [--steps K --warmup W]    # the reference's CPU engine
+
+`value` is whole-job walk-steps/s with the walks and counts resident in HBM
+(CUDA events on the launching stream, L2 flushed by a 256 MB write between
+steps, max over ranks).  `e2e` is the same metric through the C-ABI call a
+host program makes (gw_run_pools): 64-bit walk words copied from pinned host
+memory and the counts copied back, every step.  Multi-GPU: the graph is
+replicated, each rank runs its own full walk set (walk ids offset by rank,
+weak scaling) and the visit counts are summed across ranks with one NCCL
+all-reduce per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "walk-steps/s"
+FALLBACK_HBM_GBS = 6650.0
+BYTES_PER_STEP = 64  # one 32-B sector for the vertex record + one for the column id
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scale", type=int, default=24)
+    ap.add_argument("--edge-factor", type=int, default=16)
+    ap.add_argument("--L", type=int, default=10)
+    ap.add_argument("--nblocks", type=int, default=32)
+    ap.add_argument("--graph-seed", type=int, default=1)
+    ap.add_argument("--walk-seed", type=int, default=42)
+    ap.add_argument("--aggregate", type=int, default=0, help="warp-aggregated counter atomics")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-sec", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def blocksize_kb_for(scale: int, ef: int, nblocks: int) -> int:
+    return math.ceil(ef * (1 << scale) * 4 / nblocks / 1024)
+
+
+def workload_config(args, nblocks_actual=None) -> dict:
+    return {"workload": f"raw random walks, R-MAT scale {args.scale} ef {args.edge_factor}, one walk per vertex, "
+                        f"L={args.L}, jump rule, uint32 visit counts (rwdomination)",
+            "graph": f"rmat(scale={args.scale}, ef={args.edge_factor}, a=0.57, b=0.19, c=0.19, seed={args.graph_seed})",
+            "nvertices": 1 << args.scale, "walks_per_gpu": 1 << args.scale, "L": args.L,
+            "nblocks": nblocks_actual if nblocks_actual is not None else args.nblocks,
+            "blocksize_kb": blocksize_kb_for(args.scale, args.edge_factor, args.nblocks),
+            "rng": f"philox4x32-10 seed {args.walk_seed}", "l2": "flushed between steps (256 MB write)",
+            "parallelism": f"replicated graph, walks sharded, dp{args.gpus}"}
+
+
+# --------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_id: str | None):
+        self.proc = None
+        self.path = None
+        self.device_id = device_id
+
+    def __enter__(self):
+        try:
+            self.path = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"]
+            if self.device_id:
+                cmd.insert(1, f"--id={self.device_id}")
+            self.proc = subprocess.Popen(cmd, stdout=self.path, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict | None:
+        if not self.proc or not self.path:
+            return None
+        rows = []
+        for line in Path(self.path.name).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                rows.append((float(parts[0]), float(parts[1]), float(parts[2]), parts[3:]))
+            except ValueError:
+                continue
+        os.unlink(self.path.name)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[3][1:]) if v.lower().startswith("active")})
+        loaded = [r for r in rows if r[2] > 250.0] or rows
+        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": max(r[1] for r in rows),
+                "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": reasons}
+
+
+def device_uuid(dev: int) -> str | None:
+    import torch
+    try:
+        u = str(torch.cuda.get_device_properties(dev).uuid)
+        return u if u.startswith("GPU-") else f"GPU-{u}"
+    except Exception:
+        return None
+
+
+def measured_peaks() -> tuple[float, str]:
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        try:
+            return float(json.loads(f.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic() -> float | None:
+    """DRAM bytes per walk launch from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / "walk_resident_rmat24.json"
+    if f.exists():
+        try:
+            return float(json.loads(f.read_text())["dram_bytes_per_launch"])
+        except Exception:
+            return None
+    return None
+
+
+# --------------------------------------------------------------------------- reference arm
+def write_reference_graph(tmp: Path, args, rowptr, colidx) -> tuple[str, int, int]:
+    from graphwalker_b200 import formats
+    base = str(tmp / f"rmat{args.scale}")
+    kb = blocksize_kb_for(args.scale, args.edge_factor, args.nblocks)
+    blocks = formats.write_graph(base, rowptr, colidx, kb)
+    (tmp / "conf").mkdir(exist_ok=True)
+    (tmp / "conf" / "graphwalker.cnf").write_text("# GraphWalker configuration (empty)\n")
+    return base, kb, len(blocks) - 1
+
+
+def make_graph_host(args):
+    """The benchmark graph on the host: generated on the GPU when one is
+    present (input preparation only), else by the C generator."""
+    import numpy as np
+    try:
+        import torch
+        if torch.cuda.is_available():
+            import graphwalker_b200 as gw
+            with gw.Graph.rmat(args.scale, args.edge_factor, seed=args.graph_seed,
+                               blocksize_kb=blocksize_kb_for(args.scale, args.edge_factor, args.nblocks)) as G:
+                return G.export_csr()
+    except ImportError:
+        pass
+    from oracle import py_oracle
+    return py_oracle.rmat_csr(args.scale, args.edge_factor, seed=args.graph_seed)
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_ref_bench(base, kb, nv, L, stride, warmup, steps, threads, cwd) -> list[tuple[int, float]]:
+    exe = ROOT / "oracle" / "_ref" / "gw_ref_bench"
+    if not exe.exists():
+        raise FileNotFoundError(f"{exe} missing (built by `make -C oracle ref` where the reference tree exists)")
+    out = subprocess.run([str(exe), base, str(kb), str(nv), str(L), str(stride), str(warmup), str(steps),
+                          "execthreads", str(threads)], cwd=cwd, capture_output=True, text=True, timeout=1800)
+    if out.returncode != 0:
+        raise RuntimeError(f"gw_ref_bench failed ({out.returncode}): {out.stderr[-500:]}")
+    res = []
+    for line in out.stdout.splitlines():
+        f = line.split()
+        if len(f) == 8 and f[0] == "step":
+            res.append((int(f[3]) * L, float(f[7])))  # jump-rule walks make exactly L visits
+    return res
+
+
+def cpu_reference(args, rowptr, colidx, warmup: int, steps: int, budget_s: float) -> dict:
+    """Times the reference engine on the host cores; the per-run sample (one
+    walk on every `stride`-th vertex) is sized so warmup+steps runs fit budget_s."""
+    threads = host_cores()
+    with tempfile.TemporaryDirectory(prefix="gw_ref_") as td:
+        tmp = Path(td)
+        base, kb, nb = write_reference_graph(tmp, args, rowptr, colidx)
+        nv = len(rowptr) - 1
+        probe_stride = 64
+        cal = run_ref_bench(base, kb, nv, args.L, probe_stride, 1, 1, threads, tmp)
+        rate = cal[0][0] / max(cal[0][1], 1e-9)
+        per_step = budget_s / max(1, warmup + steps)
+        want_walks = max(1024, min(nv, int(rate * per_step / args.L)))
+        stride = max(1, nv // want_walks)
+        res = run_ref_bench(base, kb, nv, args.L, stride, warmup, steps, threads, tmp)
+    tot_steps = sum(s for s, _ in res)
+    tot_t = sum(t for _, t in res)
+    return {"value": tot_steps / tot_t, "unit": METRIC, "cores": threads, "kind": "reference",
+            "sec_per_step": tot_t / len(res), "steps": len(res), "nblocks": nb,
+            "sample": f"the reference engine (graphwalker.hpp) + RandomWalkwithJump compiled -O3 from source, "
+                      f"native rand_r, {threads} OpenMP threads, one walk on every {stride}-th vertex "
+                      f"({nv // stride} walks x {args.L} hops per run) of the same scale-{args.scale} graph, "
+                      f"blocks cached in RAM after the first run"}
+
+
+def reference_arm(args) -> None:
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    rowptr, colidx = make_graph_host(args)
+    warm = max(1, args.warmup)
+    r = cpu_reference(args, rowptr, colidx, warm, args.steps, budget_s=150.0)
+    line = {"metric": METRIC, "value": r["value"], "unit": METRIC, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": warm, "ms_per_step": r["sec_per_step"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": workload_config(args, r["nblocks"]),
+            "cpu_baseline": {"value": r["value"], "unit": METRIC, "cores": r["cores"], "kind": "reference",
+                             "sample": r["sample"]},
+            "e2e": {"value": r["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- this engine
+def our_arm(args) -> None:
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import graphwalker_b200 as gw
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    kb = blocksize_kb_for(args.scale, args.edge_factor, args.nblocks)
+    G = gw.Graph.rmat(args.scale, args.edge_factor, seed=args.graph_seed, blocksize_kb=kb, device=local)
+    nv, L = G.nv, args.L
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+
+    # walk records resident in HBM: one walk per vertex, ids offset by rank
+    v = torch.arange(nv, dtype=torch.int64, device="cuda")
+    walks = torch.stack([v, v + rank * nv, v, torch.zeros_like(v)], dim=1).to(torch.int32).contiguous()
+    counts = torch.zeros(nv, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    p = gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, L, seed=args.walk_seed, aggregate=bool(args.aggregate))
+
+    def step():
+        counts.zero_()
+        G.walk_device(p, walks, nv, counts=counts, stream=sh)
+
+    def barrier():
+        if world > 1:
+            dist.barrier(device_ids=[local])
+
+    for _ in range(max(3, args.warmup)):
+        step()
+        if world > 1:
+            dist.all_reduce(counts)
+    G.sync(sh)
+    total_visits = int(counts.to(torch.int64).sum().item())
+    expect = nv * L * world
+    if total_visits != expect:
+        raise RuntimeError(f"visit count {total_visits} != {expect}")
+
+    K = args.steps
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+    with ClockSampler(device_uuid(local)) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        for k in range(K):
+            flush.fill_(k & 0xFF)
+            ev[k][0].record(stream)
+            counts.zero_()
+            ev[k][1].record(stream)
+            G.walk_device(p, walks, nv, counts=counts, stream=sh)
+            ev[k][2].record(stream)
+            if world > 1:
+                dist.all_reduce(counts)
+        torch.cuda.synchronize()
+        barrier()
+    G.sync(sh)
+    step_ms = sum(e[0].elapsed_time(e[2]) for e in ev) / K
+    kern_ms = sum(e[1].elapsed_time(e[2]) for e in ev) / K
+    if world > 1:
+        t = torch.tensor([step_ms, kern_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms, kern_ms = t.tolist()
+    steps_per_launch = nv * L
+    value = steps_per_launch * world / (step_ms * 1e-3)
+
+    # random-sector gather roof: an 8 GB buffer, far larger than L2
+    gather_bps = None
+    if rank == 0:
+        buf = torch.empty(1 << 31, dtype=torch.int32, device="cuda")
+        gather_bps = G.probe_gather(buf, buf.numel(), 1 << 28, iters=5)
+        del buf
+        torch.cuda.empty_cache()
+
+    # e2e through the C-ABI host call (pinned words in, counts out)
+    e2e = None
+    if not args.no_e2e:
+        vv = np.arange(nv, dtype=np.uint64)
+        blocks = G.blocks.astype(np.int64)
+        blk = np.searchsorted(blocks[1:], np.arange(nv), side="right")
+        words_np = gw.encode(vv, vv - blocks[blk].astype(np.uint64), 0)
+        offs_np = np.r_[0, np.cumsum(np.bincount(blk, minlength=G.nblocks))].astype(np.uint64)
+        words = torch.from_numpy(words_np.view(np.int64)).pin_memory()
+        offs = torch.from_numpy(offs_np.view(np.int64)).pin_memory()
+        ids = None
+        if rank:
+            ids = torch.from_numpy((np.arange(nv, dtype=np.uint64) + rank * nv).astype(np.uint32).view(np.int32)).pin_memory()
+        hcounts = torch.zeros(nv, dtype=torch.int32).pin_memory()
+        for _ in range(3):
+            G.run_pools(p, words.data_ptr(), offs.data_ptr(), hcounts.data_ptr(), ids=None if ids is None else ids.data_ptr())
+        barrier()
+        t0 = time.perf_counter()
+        n_e2e = min(K, 50)
+        for _ in range(n_e2e):
+            G.run_pools(p, words.data_ptr(), offs.data_ptr(), hcounts.data_ptr(), ids=None if ids is None else ids.data_ptr())
+        e2e_s = (time.perf_counter() - t0) / n_e2e
+        if world > 1:
+            t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = t.item()
+        if int(hcounts.numpy().view(np.uint32).astype(np.int64).sum()) != nv * L:
+            raise RuntimeError("e2e visit count mismatch")
+        e2e = {"value": steps_per_launch * world / e2e_s, "unit": METRIC,
+               "h2d_bytes_per_step": int(words.numel() * 8 + offs.numel() * 8 + (ids.numel() * 4 if ids is not None else 0)),
+               "d2h_bytes_per_step": int(nv * 4), "ms_per_step": e2e_s * 1e3,
+               "api": "gw_run_pools (C ABI, pinned host buffers)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            rowptr, colidx = G.export_csr()
+            cpu = cpu_reference(args, rowptr, colidx, 1, 1, budget_s=args.cpu_sample_sec)
+            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as exc:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": METRIC, "cores": host_cores(), "kind": "reference",
+                   "sample": f"unavailable: {exc}"}
+
+    if world > 1:
+        dist.barrier(device_ids=[local])
+        dist.destroy_process_group()
+    if rank != 0:
+        G.close()
+        return
+    peak, peak_kind = measured_peaks()
+    achieved = BYTES_PER_STEP * steps_per_launch / (kern_ms * 1e-3) / 1e9
+    traffic = profile_traffic()
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "peak_source": f"{peak_kind} HBM copy bandwidth",
+            "bytes_per_step": BYTES_PER_STEP, "kernel": "walk_resident_kernel<JUMP, VERTEX_COUNT>",
+            "kernel_ms": kern_ms}
+    if gather_bps:
+        roof["gather_peak_gbs"] = gather_bps / 1e9
+        roof["gather_frac"] = achieved / (gather_bps / 1e9)
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
+            "warmup": max(3, args.warmup), "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": workload_config(args, G.nblocks),
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": K, "clocks": clk.summary(),
+            "walk_steps_per_step": steps_per_launch * world}
+    G.close()
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        our_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,19 @@
+"""graphwalker_b200 -- a B200 (sm_100a) engine for GraphWalker's random-walk hot path.
+
+The product is the CUDA library graphwalker_b200/lib/libgw_b200.so behind the
+C ABI in include/graphwalker_b200.h; this package is its Python handle.
+The first call into the engine loads the library and raises ImportError when
+it is missing (build it with `python -m graphwalker_b200.build`); there is no
+CPU fallback.
+"""
+from ._lib import (MODE_BLOCKED, MODE_RESIDENT, RESIDENT_HBM, RULE_JUMP, RULE_PPR, RULE_PROB,
+                   RULE_RESTART, RULE_STOP, SINK_CLOSURE_COUNT, SINK_NONE, SINK_PATH_RECORD,
+                   SINK_VERTEX_COUNT, STREAM_PINNED, GwError, WalkParams, WalkRec, load)
+from .engine import Graph, compute_blocks, encode, get_current, get_hop, get_source, params
+
+__all__ = [
+    "Graph", "GwError", "WalkParams", "WalkRec", "params", "encode", "get_source", "get_current",
+    "get_hop", "compute_blocks", "load", "RULE_JUMP", "RULE_STOP", "RULE_PROB", "RULE_RESTART",
+    "RULE_PPR", "SINK_NONE", "SINK_VERTEX_COUNT", "SINK_PATH_RECORD", "SINK_CLOSURE_COUNT",
+    "MODE_RESIDENT", "MODE_BLOCKED", "RESIDENT_HBM", "STREAM_PINNED",
+]

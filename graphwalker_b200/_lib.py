@@ -1,0 +1,121 @@
+"""ctypes binding of the C ABI declared in include/graphwalker_b200.h.
+
+The shared library is built in-tree (graphwalker_b200/lib/libgw_b200.so, see
+graphwalker_b200/build.py).  There is no fallback: if the library is missing
+the import fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import (POINTER, Structure, c_char_p, c_double, c_float, c_int32, c_size_t, c_uint32,
+                    c_uint64, c_void_p)
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libgw_b200.so"
+HEADER_PATH = Path(__file__).resolve().parent.parent / "include" / "graphwalker_b200.h"
+
+GW_OK = 0
+GW_E_INVALID, GW_E_CUDA, GW_E_NOMEM, GW_E_IO = 1, 2, 3, 4
+GW_E_BOUNDS, GW_E_OVERFLOW, GW_E_STATE, GW_E_TIMEOUT = 5, 6, 7, 8
+
+RULE_JUMP, RULE_STOP, RULE_PROB, RULE_RESTART, RULE_PPR = 0, 1, 2, 3, 4
+SINK_NONE, SINK_VERTEX_COUNT, SINK_PATH_RECORD, SINK_CLOSURE_COUNT = 0, 1, 2, 3
+MODE_RESIDENT, MODE_BLOCKED = 0, 1
+RESIDENT_HBM, STREAM_PINNED = 0, 1
+
+
+class WalkRec(Structure):
+    _fields_ = [("cur", c_uint32), ("id", c_uint32), ("src", c_uint32), ("hop", c_uint32)]
+
+
+class WalkParams(Structure):
+    _fields_ = [("rule", c_uint32), ("sink", c_uint32), ("L", c_uint32), ("njump", c_uint32),
+                ("jump_prob", c_double), ("seed", c_uint64), ("mode", c_uint32),
+                ("path_stride", c_uint32), ("max_hops", c_uint32), ("prob", c_float),
+                ("aggregate", c_uint32), ("max_supersteps", c_uint32), ("reserved", c_uint32 * 6)]
+
+
+class RunStats(Structure):
+    _fields_ = [("walks", c_uint64), ("supersteps", c_uint64), ("block_loads", c_uint64),
+                ("bytes_h2d", c_uint64), ("ms_total", c_double), ("ms_walk", c_double),
+                ("ms_partition", c_double), ("ms_copy_wait", c_double)]
+
+
+class GraphDesc(Structure):
+    _fields_ = [("base_filename", c_char_p), ("blocksize_kb", c_uint64), ("nmblocks", c_uint32),
+                ("residency", c_uint32), ("device", c_int32)]
+
+
+class GwError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"gw status {code}: {msg}")
+        self.code = code
+
+
+_P = c_void_p
+_SIGS = {
+    "gw_version": (c_char_p, []),
+    "gw_encode": (c_uint64, [c_uint32, c_uint32, c_uint32]),
+    "gw_get_source": (c_uint32, [c_uint64]),
+    "gw_get_current": (c_uint32, [c_uint64]),
+    "gw_get_hop": (c_uint32, [c_uint64]),
+    "gw_continue_threshold": (c_uint32, [c_double]),
+    "gw_getblock": (c_uint32, [_P, c_uint32, c_uint32]),
+    "gw_compute_blocks": (c_uint32, [_P, c_uint32, c_uint64, _P, c_uint32]),
+    "gw_comp_block_size": (c_uint64, [c_uint64]),
+    "gw_comp_nmblocks": (c_uint32, [c_uint64, c_uint64]),
+    "gw_open": (c_int32, [POINTER(GraphDesc), POINTER(c_void_p)]),
+    "gw_open_csr": (c_int32, [_P, _P, c_uint32, _P, c_uint32, c_uint32, c_int32, POINTER(c_void_p)]),
+    "gw_open_rmat": (c_int32, [c_uint32, c_uint32, c_uint64, c_double, c_double, c_double, c_uint64,
+                               c_int32, POINTER(c_void_p)]),
+    "gw_close": (c_int32, [_P]),
+    "gw_last_error": (c_char_p, [_P]),
+    "gw_graph_info": (c_int32, [_P, POINTER(c_uint32), POINTER(c_uint64), POINTER(c_uint32)]),
+    "gw_get_blocks": (c_int32, [_P, _P, c_uint32]),
+    "gw_export_csr": (c_int32, [_P, _P, _P]),
+    "gw_walks_clear": (c_int32, [_P]),
+    "gw_walks_add": (c_int32, [_P, c_uint32, _P, _P, c_size_t]),
+    "gw_walks_count": (c_int32, [_P, _P, POINTER(c_uint64)]),
+    "gw_run": (c_int32, [_P, POINTER(WalkParams)]),
+    "gw_read_counts": (c_int32, [_P, _P, c_size_t]),
+    "gw_read_paths": (c_int32, [_P, _P, _P, c_size_t]),
+    "gw_read_closure": (c_int32, [_P, POINTER(c_uint64)]),
+    "gw_read_stats": (c_int32, [_P, POINTER(RunStats)]),
+    "gw_read_pool": (c_int32, [_P, c_uint32, _P, c_size_t, POINTER(c_uint64)]),
+    "gw_run_pools": (c_int32, [_P, POINTER(WalkParams), _P, _P, _P, _P]),
+    "gw_walk_device": (c_int32, [_P, POINTER(WalkParams), _P, c_uint64, _P, _P, _P, _P, _P]),
+    "gw_unpack_words_device": (c_int32, [_P, c_uint32, _P, _P, c_uint64, _P, _P]),
+    "gw_pack_words_device": (c_int32, [_P, _P, c_uint64, _P, _P, _P]),
+    "gw_sync": (c_int32, [_P, _P]),
+    "gw_probe_gather": (c_int32, [_P, _P, c_uint64, c_uint64, ctypes.c_int, POINTER(c_double)]),
+}
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Loads libgw_b200.so and declares every entry point; raises if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m graphwalker_b200.build` "
+            "(the engine has no CPU fallback)")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(status: int, ctx=None) -> None:
+    if status != GW_OK:
+        msg = load().gw_last_error(ctx)
+        raise GwError(status, msg.decode() if msg else "")
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGS)

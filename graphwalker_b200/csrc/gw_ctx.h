@@ -1,0 +1,135 @@
+// gw_ctx.h -- the engine context behind the C ABI (one per graph).
+#pragma once
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "gw_internal.h"
+
+// A device allocation owned by the context.
+struct gw_devbuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t n) {
+    if (n <= bytes && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&p, n ? n : 16);
+    if (e == cudaSuccess) bytes = n;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+// A pinned host allocation owned by the context.
+struct gw_hostbuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t n) {
+    if (n <= bytes && p) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaHostAlloc(&p, n ? n : 16, cudaHostAllocDefault);
+    if (e == cudaSuccess) bytes = n;
+    return e;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+struct gw_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;       // compute stream
+  cudaStream_t copy_stream = nullptr;  // block / walk copies
+  uint32_t residency = GW_RESIDENT_HBM;
+  uint32_t nmblocks = 2;
+
+  // graph
+  uint32_t nv = 0;
+  uint64_t ne = 0;
+  uint32_t nblocks = 0;
+  std::vector<uint32_t> blocks;  // nblocks + 1
+  gw_devbuf d_rowptr, d_colidx, d_vrec, d_blocks;
+  gw_hostbuf h_rowptr, h_colidx;  // pinned copy (streaming residency)
+
+  // device status word (+ pinned mirror)
+  gw_devbuf d_status;
+  gw_hostbuf h_status;
+
+  // walk pools on the host side (WalkManager::pwalks analogue before upload)
+  std::vector<std::vector<uint64_t>> pool_words;
+  std::vector<std::vector<uint32_t>> pool_ids;
+  bool pools_have_ids = false;
+
+  // run outputs
+  gw_devbuf d_walks, d_words, d_ids, d_counts, d_paths, d_plen, d_closure, d_pool_offsets;
+  uint64_t last_nwalks = 0;
+  uint32_t last_stride = 0;
+  uint32_t last_sink = GW_SINK_NONE;
+  bool have_run = false;
+  gw_run_stats stats{};
+
+  // blocked engine scratch
+  gw_devbuf d_dest, d_tile_hist, d_tile_off, d_totals, d_minhop, d_scan_temp, d_out_ptr,
+      d_out_base;
+  std::vector<gw_devbuf> pools;   // per-block device pools
+  std::vector<uint64_t> pool_size;
+  std::vector<uint32_t> minstep;  // per-block min hop (WalkManager::minstep)
+
+  std::string err;
+
+  gw_status fail(gw_status code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    err = buf;
+    return code;
+  }
+  gw_status cuda_fail(cudaError_t e, const char* what) {
+    return fail(GW_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  }
+  gw::GraphView view() const {
+    gw::GraphView g;
+    g.vrec = d_vrec.as<const unsigned long long>();
+    g.rowptr = d_rowptr.as<const unsigned long long>();
+    g.colidx = d_colidx.as<const uint32_t>();
+    g.nv = nv;
+    return g;
+  }
+};
+
+namespace gw {
+// Fills launch constants from the API parameters; validates them.
+gw_status make_walk_args(gw_ctx* ctx, const gw_walk_params* p, WalkArgs* a);
+// Reads and clears the device status word (synchronises ctx->stream).
+gw_status take_status(gw_ctx* ctx, cudaStream_t stream);
+// GraphWalker's block loop on the device (gw_engine.cu).
+gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p);
+}  // namespace gw
+
+#define GW_CUDA(ctx, expr, what)                    \
+  do {                                              \
+    cudaError_t _e = (expr);                        \
+    if (_e != cudaSuccess) return (ctx)->cuda_fail(_e, what); \
+  } while (0)

@@ -1,0 +1,179 @@
+// gw_device.cuh -- device-side building blocks of the walk engine.
+//
+// Per-hop draws: words 0 and 1 of Philox4x32-10 (Salmon et al., SC'11) with
+// key = seed and counter = (walk id, hop, 0, 0), each shifted right by one so
+// that they span rand_r's [0, RAND_MAX] (src/api/datatype.hpp:8).  The draw
+// consumption order is the reference's (randomwalkwithjump.hpp:45-50): when
+// the vertex has out-edges the first word is the continuation test and the
+// second picks the neighbour (or the jump target when the test fails); a
+// dangling vertex skips the test (short-circuit `outd > 0 && ...`) and its
+// jump uses the first word.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/graphwalker_b200.h"
+
+namespace gw {
+
+// Packed vertex record: (first-edge offset << 24) | min(out-degree, 0xFFFFFF).
+// One 8-byte load (always inside one 32-byte sector) replaces the two 8-byte
+// row-pointer loads; a degree field of 0xFFFFFF means "read the row pointer".
+constexpr uint32_t kDegEscape = 0xFFFFFFu;
+constexpr int kDegBits = 24;
+
+constexpr uint32_t kPhiloxM0 = 0xD2511F53u;
+constexpr uint32_t kPhiloxM1 = 0xCD9E8D57u;
+constexpr uint32_t kPhiloxW0 = 0x9E3779B9u;
+constexpr uint32_t kPhiloxW1 = 0xBB67AE85u;
+
+struct Philox4 {
+  uint32_t x, y, z, w;
+};
+
+__host__ __device__ __forceinline__ Philox4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2,
+                                                         uint32_t c3, uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint64_t p0 = (uint64_t)kPhiloxM0 * c0;
+    const uint64_t p1 = (uint64_t)kPhiloxM1 * c2;
+    const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+    const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+    c0 = n0;
+    c1 = (uint32_t)p1;
+    c2 = n2;
+    c3 = (uint32_t)p0;
+    k0 += kPhiloxW0;
+    k1 += kPhiloxW1;
+  }
+  return Philox4{c0, c1, c2, c3};
+}
+
+// Launch-constant parameters of a walk kernel (passed by value, lands in the
+// constant bank).
+struct WalkArgs {
+  uint32_t L;          // length cap (JUMP/STOP/PPR) or segment length (RESTART)
+  uint32_t thr;        // continuation passes iff draw >= thr
+  uint32_t njump;      // JUMP target range
+  uint32_t max_hops;   // hop guard of the uncapped rule
+  uint32_t seed_lo, seed_hi;
+  uint32_t path_stride;
+  uint32_t lo, hi;     // block range [lo, hi) in blocked mode
+};
+
+struct GraphView {
+  const unsigned long long* __restrict__ vrec;    // packed vertex records (nv)
+  const unsigned long long* __restrict__ rowptr;  // row pointer (nv + 1)
+  const uint32_t* __restrict__ colidx;
+  uint32_t nv;
+};
+
+struct SinkView {
+  uint32_t* __restrict__ counts;             // VERTEX_COUNT
+  uint32_t* __restrict__ paths;              // PATH_RECORD, [walk][visit]
+  uint32_t* __restrict__ plen;               // PATH_RECORD, visits per walk
+  unsigned long long* __restrict__ closure;  // CLOSURE_COUNT
+};
+
+template <int RULE>
+__device__ __forceinline__ constexpr bool rule_capped() {
+  return RULE == GW_RULE_JUMP || RULE == GW_RULE_STOP || RULE == GW_RULE_PPR;
+}
+
+// One hop of one walk at vertex v (already visited).  Returns false when the
+// walk ends inside this hop (stop rules); otherwise v is the next vertex and
+// the caller increments the hop.  Loads go through the read-only path.
+template <int RULE>
+__device__ __forceinline__ bool hop_advance(const GraphView& g, const WalkArgs& a, uint32_t id,
+                                            uint32_t src, uint32_t hop, uint32_t& v) {
+  const unsigned long long rec = __ldg(g.vrec + v);
+  const Philox4 ph = philox4x32_10(id, hop, 0u, 0u, a.seed_lo, a.seed_hi);
+  const uint32_t d0 = ph.x >> 1;
+  const uint32_t d1 = ph.y >> 1;
+  unsigned long long off = rec >> kDegBits;
+  unsigned long long deg = rec & kDegEscape;
+  if (deg == kDegEscape) {  // mega-hub: exact degree from the row pointer
+    const unsigned long long b = __ldg(g.rowptr + v);
+    deg = __ldg(g.rowptr + v + 1) - b;
+    off = b;
+  }
+  if (deg > 0 && d0 >= a.thr) {
+    // (eid_t)rand_r % outd with a 31-bit draw: equals the draw when outd > 2^31
+    const unsigned long long r =
+        deg > 0x7fffffffull ? (unsigned long long)d1 : (unsigned long long)(d1 % (uint32_t)deg);
+    v = __ldg(g.colidx + off + r);
+    return true;
+  }
+  const uint32_t dj = deg > 0 ? d1 : d0;
+  if (RULE == GW_RULE_JUMP) {
+    v = dj % a.njump;
+    return true;
+  } else if (RULE == GW_RULE_RESTART) {
+    v = src;
+    return true;
+  } else if (RULE == GW_RULE_PPR) {
+    if (deg == 0) {
+      v = src;
+      return true;
+    }
+    return false;
+  }
+  return false;  // STOP, PROB
+}
+
+// Same hop over a block-local CSR slice (streamed blocks): beg_pos is the
+// slice of the row pointer for [lo, hi] (global edge offsets) and csr the
+// slice of the column array that starts at beg_pos[0], exactly the buffers
+// the reference's loadSubGraph fills (graphwalker.hpp:168-209).
+template <int RULE>
+__device__ __forceinline__ bool hop_advance_slice(const unsigned long long* __restrict__ beg_pos,
+                                                  const uint32_t* __restrict__ csr,
+                                                  const WalkArgs& a, uint32_t id, uint32_t src,
+                                                  uint32_t hop, uint32_t& v) {
+  const uint32_t vl = v - a.lo;
+  const unsigned long long b0 = __ldg(beg_pos);
+  const unsigned long long b = __ldg(beg_pos + vl);
+  const unsigned long long deg = __ldg(beg_pos + vl + 1) - b;
+  const Philox4 ph = philox4x32_10(id, hop, 0u, 0u, a.seed_lo, a.seed_hi);
+  const uint32_t d0 = ph.x >> 1;
+  const uint32_t d1 = ph.y >> 1;
+  if (deg > 0 && d0 >= a.thr) {
+    const unsigned long long r =
+        deg > 0x7fffffffull ? (unsigned long long)d1 : (unsigned long long)(d1 % (uint32_t)deg);
+    v = __ldg(csr + (b - b0) + r);
+    return true;
+  }
+  const uint32_t dj = deg > 0 ? d1 : d0;
+  if (RULE == GW_RULE_JUMP) {
+    v = dj % a.njump;
+    return true;
+  } else if (RULE == GW_RULE_RESTART) {
+    v = src;
+    return true;
+  } else if (RULE == GW_RULE_PPR) {
+    if (deg == 0) {
+      v = src;
+      return true;
+    }
+    return false;
+  }
+  return false;
+}
+
+// Count one visit of v.  AGG folds lanes of the warp that visit the same
+// vertex in the same instruction into one atomic (hub vertices, and every
+// walk of a single-source query at hop 0).
+template <bool AGG>
+__device__ __forceinline__ void count_visit(uint32_t* __restrict__ counts, uint32_t v) {
+  if (AGG) {
+    const unsigned active = __activemask();
+    const unsigned peers = __match_any_sync(active, v);
+    const int lane = threadIdx.x & 31;
+    if (lane == __ffs(peers) - 1) atomicAdd(counts + v, (uint32_t)__popc(peers));
+  } else {
+    atomicAdd(counts + v, 1u);
+  }
+}
+
+}  // namespace gw

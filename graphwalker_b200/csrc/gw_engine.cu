@@ -1,0 +1,334 @@
+// gw_engine.cu -- GraphWalker's block loop on the device.
+//
+//   graphwalker_engine::run            src/engine/graphwalker.hpp:272-311
+//   findSubGraph / loadSubGraph        src/engine/graphwalker.hpp:168-234
+//   swapOut (evict fewest walks)       src/engine/graphwalker.hpp:236-251
+//   WalkManager::chooseBlock & co.     src/walks/walk.hpp:204-252
+//   getCurrentWalks / updateWalkNum    src/walks/walk.hpp:114-192
+//
+// Each superstep picks a block with the reference's state-aware policy (with
+// probability `prob` the block holding the lowest-hop walk, otherwise the
+// block with the most pending walks), makes its CSR available (resident HBM,
+// or a slot filled from pinned host memory by async copies on a side stream,
+// prefetching the next likely block while the current one runs), advances
+// every walk of its pool while it stays inside the block, and stably
+// partitions the walks that left into the pools of their new blocks.  The
+// per-block pending counts and minimum hops the policy reads come back from
+// the partition's histogram each superstep.
+#include <algorithm>
+#include <cstring>
+
+#include "gw_ctx.h"
+
+namespace gw {
+
+namespace {
+
+constexpr uint32_t kNoBlock = 0xffffffffu;
+
+struct Slots {
+  // One device slot holds the CSR slice of one block:
+  //   beg_pos[blocks[b] .. blocks[b+1]] and csr[beg_pos[blocks[b]] .. beg_pos[blocks[b+1]]).
+  std::vector<gw_devbuf> beg_pos, csr;
+  std::vector<uint32_t> block;      // block held, kNoBlock if empty
+  std::vector<cudaEvent_t> ready;   // copy finished
+  std::vector<cudaEvent_t> free_ev; // last kernel reading the slot finished
+  std::vector<int> slot_of;         // per block: slot index or -1
+  ~Slots() {
+    for (auto& b : beg_pos) b.release();
+    for (auto& b : csr) b.release();
+    for (auto e : ready) cudaEventDestroy(e);
+    for (auto e : free_ev) cudaEventDestroy(e);
+  }
+};
+
+// chooseBlock (walk.hpp:245-252) over the engine's pending counts.
+uint32_t block_with_max_walks(const std::vector<uint64_t>& walknum) {
+  uint64_t maxw = 0;
+  uint32_t maxp = 0;
+  for (uint32_t p = 0; p < walknum.size(); ++p)
+    if (maxw < walknum[p]) {
+      maxw = walknum[p];
+      maxp = p;
+    }
+  return maxp;
+}
+
+uint32_t block_with_min_step(const std::vector<uint64_t>& walknum, const std::vector<uint32_t>& minstep) {
+  uint32_t mins = 0xffff, minp = 0;
+  for (uint32_t p = 0; p < minstep.size(); ++p)
+    if (mins > minstep[p]) {
+      mins = minstep[p];
+      minp = p;
+    }
+  if (walknum[minp] > 0) return minp;
+  return block_with_max_walks(walknum);
+}
+
+uint32_t choose_block(const std::vector<uint64_t>& walknum, const std::vector<uint32_t>& minstep,
+                      float prob, uint64_t seed, uint64_t superstep) {
+  // the reference's coin is ((float)rand())/RAND_MAX; here its 31-bit draw
+  // comes from Philox(seed, (superstep, "CHOS")) so a run is reproducible
+  const Philox4 ph = philox4x32_10((uint32_t)superstep, (uint32_t)(superstep >> 32), 0x43484F53u,
+                                   0u, (uint32_t)seed, (uint32_t)(seed >> 32));
+  const float cc = (float)(int32_t)(ph.x >> 1) / 2147483647;
+  if (cc < prob) return block_with_min_step(walknum, minstep);
+  return block_with_max_walks(walknum);
+}
+
+}  // namespace
+
+gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
+  WalkArgs a;
+  gw_status s = make_walk_args(ctx, p, &a);
+  if (s != GW_OK) return s;
+  if (p->sink == GW_SINK_PATH_RECORD)
+    return ctx->fail(GW_E_INVALID, "PATH_RECORD needs GW_MODE_RESIDENT");
+  const uint32_t nb = ctx->nblocks;
+  if (nb + 1 > 8000) return ctx->fail(GW_E_INVALID, "at most 7999 blocks in blocked mode");
+  const bool streaming = ctx->residency == GW_STREAM_PINNED;
+  cudaStream_t st = ctx->stream, xs = ctx->copy_stream;
+
+  // ---- initial pools (startWalks; getCurrentWalks reads them back) ----
+  ctx->pools.resize(nb);
+  ctx->pool_size.assign(nb, 0);
+  ctx->minstep.assign(nb, 0xffff);
+  std::vector<uint64_t> cap(nb, 0);
+  for (uint32_t b = 0; b < nb; ++b) cap[b] = ctx->pools[b].bytes / sizeof(gw_walk_rec);
+  uint64_t walksum = 0, maxpool = 0;
+  for (uint32_t b = 0; b < nb; ++b) maxpool = std::max<uint64_t>(maxpool, ctx->pool_words[b].size());
+  GW_CUDA(ctx, ctx->d_words.ensure(maxpool * 8), "word alloc");
+  if (ctx->pools_have_ids) GW_CUDA(ctx, ctx->d_ids.ensure(maxpool * 4), "id alloc");
+  for (uint32_t b = 0; b < nb; ++b) {
+    const uint64_t m = ctx->pool_words[b].size();
+    if (!m) continue;
+    if (cap[b] < m) {
+      GW_CUDA(ctx, ctx->pools[b].ensure(m * sizeof(gw_walk_rec)), "pool alloc");
+      cap[b] = m;
+    }
+    GW_CUDA(ctx, cudaMemcpyAsync(ctx->d_words.p, ctx->pool_words[b].data(), m * 8,
+                                 cudaMemcpyHostToDevice, st), "walk upload");
+    if (ctx->pools_have_ids)
+      GW_CUDA(ctx, cudaMemcpyAsync(ctx->d_ids.p, ctx->pool_ids[b].data(), m * 4,
+                                   cudaMemcpyHostToDevice, st), "id upload");
+    GW_CUDA(ctx, launch_unpack_words(ctx->d_words.as<uint64_t>(),
+                                     ctx->pools_have_ids ? ctx->d_ids.as<uint32_t>() : nullptr, m,
+                                     ctx->blocks[b], ctx->pools[b].as<gw_walk_rec>(), st), "unpack");
+    GW_CUDA(ctx, cudaStreamSynchronize(st), "walk upload");  // host words are reused next block
+    ctx->pool_size[b] = m;
+    for (uint64_t w : ctx->pool_words[b]) ctx->minstep[b] = std::min<uint32_t>(ctx->minstep[b], gw_get_hop(w));
+    walksum += m;
+  }
+  const uint64_t nwalks = walksum;
+
+  // ---- sinks ----
+  SinkView sv{};
+  GW_CUDA(ctx, ctx->d_counts.ensure((size_t)ctx->nv * 4), "counts alloc");
+  GW_CUDA(ctx, cudaMemsetAsync(ctx->d_counts.p, 0, (size_t)ctx->nv * 4, st), "counts clear");
+  GW_CUDA(ctx, ctx->d_closure.ensure(8), "closure alloc");
+  GW_CUDA(ctx, cudaMemsetAsync(ctx->d_closure.p, 0, 8, st), "closure clear");
+  sv.counts = ctx->d_counts.as<uint32_t>();
+  sv.closure = ctx->d_closure.as<unsigned long long>();
+
+  // ---- partition scratch ----
+  const uint32_t nbk = nb + 1;  // + the "ended" bucket
+  GW_CUDA(ctx, ctx->d_totals.ensure(2 * nbk * 4), "totals alloc");  // totals | minhop
+  GW_CUDA(ctx, ctx->d_out_ptr.ensure(nbk * sizeof(void*)), "ptr alloc");
+  GW_CUDA(ctx, ctx->d_out_base.ensure(nbk * 8), "base alloc");
+  gw_hostbuf h_xfer;  // pinned: totals|minhop down, ptr|base up
+  GW_CUDA(ctx, h_xfer.ensure(2 * nbk * 4 + nbk * (sizeof(void*) + 8)), "pinned scratch");
+  uint32_t* h_totals = h_xfer.as<uint32_t>();
+  uint32_t* h_minhop = h_totals + nbk;
+  gw_walk_rec** h_ptr = reinterpret_cast<gw_walk_rec**>(h_totals + 2 * nbk);
+  uint64_t* h_base = reinterpret_cast<uint64_t*>(h_ptr + nbk);
+
+  // ---- streamed block slots ----
+  Slots slots;
+  const uint32_t nslots = streaming ? std::max<uint32_t>(2, std::min(ctx->nmblocks, nb)) : 0;
+  if (streaming) {
+    uint64_t max_v = 0, max_e = 0;
+    const uint64_t* hr = ctx->h_rowptr.as<uint64_t>();
+    for (uint32_t b = 0; b < nb; ++b) {
+      max_v = std::max<uint64_t>(max_v, ctx->blocks[b + 1] - ctx->blocks[b]);
+      max_e = std::max<uint64_t>(max_e, hr[ctx->blocks[b + 1]] - hr[ctx->blocks[b]]);
+    }
+    slots.beg_pos.resize(nslots);
+    slots.csr.resize(nslots);
+    slots.block.assign(nslots, kNoBlock);
+    slots.ready.resize(nslots);
+    slots.free_ev.resize(nslots);
+    slots.slot_of.assign(nb, -1);
+    for (uint32_t i = 0; i < nslots; ++i) {
+      GW_CUDA(ctx, slots.beg_pos[i].ensure((max_v + 1) * 8), "slot alloc");
+      GW_CUDA(ctx, slots.csr[i].ensure(std::max<uint64_t>(max_e, 1) * 4), "slot alloc");
+      cudaEventCreateWithFlags(&slots.ready[i], cudaEventDisableTiming);
+      cudaEventCreateWithFlags(&slots.free_ev[i], cudaEventDisableTiming);
+      cudaEventRecord(slots.free_ev[i], st);
+    }
+  }
+  ctx->stats = gw_run_stats{};
+  ctx->stats.walks = nwalks;
+
+  // findSubGraph: make block b resident in a slot (never the slot `keep`).
+  auto load_block = [&](uint32_t b, int keep) -> int {
+    if (slots.slot_of[b] >= 0) return slots.slot_of[b];
+    int victim = -1;
+    for (uint32_t i = 0; i < nslots && victim < 0; ++i)
+      if (slots.block[i] == kNoBlock && (int)i != keep) victim = (int)i;
+    if (victim < 0) {  // swapOut: resident block with the fewest pending walks
+      uint64_t minw = ~0ull;
+      for (uint32_t i = 0; i < nslots; ++i) {
+        if ((int)i == keep) continue;
+        const uint64_t w = ctx->pool_size[slots.block[i]];
+        if (w < minw) {
+          minw = w;
+          victim = (int)i;
+        }
+      }
+      slots.slot_of[slots.block[victim]] = -1;
+    }
+    const uint64_t* hr = ctx->h_rowptr.as<uint64_t>();
+    const uint32_t v0 = ctx->blocks[b], v1 = ctx->blocks[b + 1];
+    const uint64_t e0 = hr[v0], e1 = hr[v1];
+    cudaStreamWaitEvent(xs, slots.free_ev[victim], 0);
+    cudaMemcpyAsync(slots.beg_pos[victim].p, hr + v0, ((uint64_t)v1 - v0 + 1) * 8,
+                    cudaMemcpyHostToDevice, xs);
+    if (e1 > e0)
+      cudaMemcpyAsync(slots.csr[victim].p, ctx->h_colidx.as<uint32_t>() + e0, (e1 - e0) * 4,
+                      cudaMemcpyHostToDevice, xs);
+    cudaEventRecord(slots.ready[victim], xs);
+    slots.block[victim] = b;
+    slots.slot_of[b] = victim;
+    ctx->stats.block_loads++;
+    ctx->stats.bytes_h2d += ((uint64_t)v1 - v0 + 1) * 8 + (e1 - e0) * 4;
+    return victim;
+  };
+
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  cudaEventRecord(t0, st);
+  uint64_t superstep = 0;
+  cudaError_t e = cudaSuccess;
+  while (walksum > 0 && e == cudaSuccess &&
+         (p->max_supersteps == 0 || superstep < p->max_supersteps)) {
+    const uint32_t b = choose_block(ctx->pool_size, ctx->minstep, p->prob, p->seed, superstep);
+    const uint64_t n = ctx->pool_size[b];
+    if (n == 0) return ctx->fail(GW_E_STATE, "scheduler chose an empty block (walksum %llu)",
+                                 (unsigned long long)walksum);
+    WalkArgs ab = a;
+    ab.lo = ctx->blocks[b];
+    ab.hi = ctx->blocks[b + 1];
+    const unsigned long long* beg_pos = nullptr;
+    const uint32_t* csr = nullptr;
+    int slot = -1;
+    if (streaming) {
+      slot = load_block(b, -1);
+      cudaStreamWaitEvent(st, slots.ready[slot], 0);
+      beg_pos = slots.beg_pos[slot].as<unsigned long long>();
+      csr = slots.csr[slot].as<uint32_t>();
+    }
+    // ---- exec_updates ----
+    GW_CUDA(ctx, ctx->d_dest.ensure(n * 4), "dest alloc");
+    e = launch_walk_block((int)p->rule, (int)p->sink, p->aggregate != 0, ctx->pools[b].as<gw_walk_rec>(),
+                          n, ctx->view(), beg_pos, csr, ab, sv, ctx->d_blocks.as<uint32_t>(), nb,
+                          ctx->d_dest.as<uint32_t>(), ctx->d_status.as<uint32_t>(), st);
+    if (e != cudaSuccess) break;
+    if (streaming) {
+      cudaEventRecord(slots.free_ev[slot], st);
+      // prefetch the block most likely chosen next while this one runs
+      uint64_t best = 0;
+      uint32_t nxt = kNoBlock;
+      for (uint32_t q = 0; q < nb; ++q)
+        if (q != b && ctx->pool_size[q] > best) {
+          best = ctx->pool_size[q];
+          nxt = q;
+        }
+      if (nxt != kNoBlock && slots.slot_of[nxt] < 0 && nslots > 1) load_block(nxt, slot);
+    }
+    // ---- moveWalk: stable partition by destination block ----
+    const PartitionPlan plan = partition_plan(n, nbk);
+    const size_t hist_n = (size_t)plan.nbuckets * plan.ntiles;
+    GW_CUDA(ctx, ctx->d_tile_hist.ensure(hist_n * 4), "hist alloc");
+    GW_CUDA(ctx, ctx->d_tile_off.ensure(hist_n * 4), "hist alloc");
+    GW_CUDA(ctx, ctx->d_scan_temp.ensure(plan.scan_temp_bytes), "scan alloc");
+    uint32_t* d_tot = ctx->d_totals.as<uint32_t>();
+    uint32_t* d_minhop = d_tot + nbk;
+    GW_CUDA(ctx, cudaMemsetAsync(d_minhop, 0xff, nbk * 4, st), "minhop clear");
+    e = launch_partition_hist(ctx->pools[b].as<gw_walk_rec>(), ctx->d_dest.as<uint32_t>(), n, plan,
+                              ctx->d_tile_hist.as<uint32_t>(), d_minhop, st);
+    if (e == cudaSuccess)
+      e = launch_partition_scan(ctx->d_tile_hist.as<uint32_t>(), ctx->d_tile_off.as<uint32_t>(), d_tot,
+                                plan, ctx->d_scan_temp.p, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(h_totals, d_tot, 2 * nbk * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) break;
+    // updateWalkNum: grow destination pools, then scatter into them
+    for (uint32_t d = 0; d < nb; ++d) {
+      const uint64_t need = ctx->pool_size[d] + h_totals[d];
+      if (d != b && need > cap[d]) {
+        uint64_t ncap = std::max<uint64_t>(need, cap[d] * 2);
+        ncap = std::max<uint64_t>(ncap, 1024);
+        void* np = nullptr;
+        e = cudaMalloc(&np, ncap * sizeof(gw_walk_rec));
+        if (e != cudaSuccess) break;
+        if (ctx->pool_size[d])
+          e = cudaMemcpyAsync(np, ctx->pools[d].p, ctx->pool_size[d] * sizeof(gw_walk_rec),
+                              cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (ctx->pools[d].p) cudaFree(ctx->pools[d].p);
+        ctx->pools[d].p = np;
+        ctx->pools[d].bytes = ncap * sizeof(gw_walk_rec);
+        cap[d] = ncap;
+      }
+      h_ptr[d] = ctx->pools[d].as<gw_walk_rec>();
+      h_base[d] = ctx->pool_size[d];
+    }
+    if (e != cudaSuccess) break;
+    h_ptr[nb] = nullptr;
+    h_base[nb] = 0;
+    e = cudaMemcpyAsync(ctx->d_out_ptr.p, h_ptr, nbk * sizeof(void*), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(ctx->d_out_base.p, h_base, nbk * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = launch_partition_scatter(ctx->pools[b].as<gw_walk_rec>(), ctx->d_dest.as<uint32_t>(), n, plan,
+                                   ctx->d_tile_off.as<uint32_t>(),
+                                   ctx->d_out_ptr.as<gw_walk_rec* const>(),
+                                   ctx->d_out_base.as<uint64_t>(), st);
+    if (e != cudaSuccess) break;
+    // the pinned up-copies must land before h_ptr/h_base are rewritten
+    e = cudaStreamSynchronize(st);
+    uint64_t forwarded = 0;
+    for (uint32_t d = 0; d < nb; ++d) {
+      if (!h_totals[d]) continue;
+      ctx->pool_size[d] += h_totals[d];
+      forwarded += h_totals[d];
+      ctx->minstep[d] = std::min<uint32_t>(ctx->minstep[d], std::min<uint32_t>(h_minhop[d], 0xffff));
+    }
+    walksum = walksum - n + forwarded;
+    ctx->pool_size[b] = 0;
+    ctx->minstep[b] = 0xffff;
+    ++superstep;
+  }
+  cudaEventRecord(t1, st);
+  if (e != cudaSuccess) {
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return ctx->cuda_fail(e, "blocked engine");
+  }
+  s = take_status(ctx, st);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  ctx->stats.supersteps = superstep;
+  ctx->stats.ms_total = ms;
+  ctx->last_nwalks = nwalks;
+  ctx->last_sink = p->sink;
+  ctx->last_stride = 0;
+  ctx->have_run = true;
+  return s;
+}
+
+}  // namespace gw

@@ -1,0 +1,213 @@
+/*
+ * graphwalker_b200.h -- C ABI of the B200 random-walk engine.
+ *
+ * This is the thin boundary between GraphWalker-style host programs (the
+ * drop-in C++ headers under graphwalker_b200/compat, a cgo/JNI/ctypes
+ * binding, the Python tests) and the sm_100a kernels.  Plain pointers and
+ * sizes only.
+ *
+ * Ownership: a gw_ctx owns every device buffer it allocates; the caller owns
+ * every host buffer it passes, and no pointer is retained past the call that
+ * received it.  *_device entry points take device pointers and a CUDA
+ * stream (cudaStream_t passed as void*, NULL = the context's stream) and are
+ * stream-ordered: they return once the work is enqueued.
+ * Errors: every call returns a gw_status (0 = GW_OK).  Device-side
+ * violations (an out-of-range vertex id, a full sink) are reported through a
+ * device status word and surface as GW_E_BOUNDS / GW_E_OVERFLOW from the
+ * next synchronising call; kernels never trap.  gw_last_error() gives text.
+ * Threading: one context per host thread; calls on one context are not
+ * reentrant.
+ *
+ * Reference interfaces replaced (GraphWalker, paths in its project root):
+ *   graphwalker_engine ctor + run()      src/engine/graphwalker.hpp:74-126, 272-311
+ *   WalkManager (pools, codec, counts)   src/walks/walk.hpp:17-267
+ *   RandomWalk*::updateByWalk            src/walks/randomwalk*.hpp
+ *   convert_if_notexists / compute_block src/preprocess/conversions.hpp:300-404
+ */
+#ifndef GRAPHWALKER_B200_H
+#define GRAPHWALKER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t gw_status;
+typedef struct gw_ctx gw_ctx;
+
+#define GW_OK 0
+#define GW_E_INVALID 1  /* bad argument                                  */
+#define GW_E_CUDA 2     /* a CUDA runtime call failed                    */
+#define GW_E_NOMEM 3    /* device or pinned allocation failed            */
+#define GW_E_IO 4       /* graph file missing / short read               */
+#define GW_E_BOUNDS 5   /* a kernel met a vertex id >= nvertices         */
+#define GW_E_OVERFLOW 6 /* a sink ran out of room (path stride, table)   */
+#define GW_E_STATE 7    /* call not valid in the context's state         */
+#define GW_E_TIMEOUT 8  /* a bounded device wait gave up                 */
+
+/* Walk update rules: the else-branch of the per-hop continuation test. */
+#define GW_RULE_JUMP 0    /* RandomWalkwithJump: jump to rand % N, cap L          */
+#define GW_RULE_STOP 1    /* RandomWalkwithStop: terminate, cap L                 */
+#define GW_RULE_PROB 2    /* RandomWalkwithProb: terminate, no cap                */
+#define GW_RULE_RESTART 3 /* RandomWalkwithRestartwithJoint: back to source,
+                             segment ends when hop % L == L-1                     */
+#define GW_RULE_PPR 4     /* terminate; a dangling vertex sends the walk back to
+                             its source; cap L (single-source PPR workload)       */
+
+/* Visit sinks: what the engine accumulates per visit (the app's updateInfo). */
+#define GW_SINK_NONE 0         /* rawrandomwalks                                  */
+#define GW_SINK_VERTEX_COUNT 1 /* rwdomination: counts[v] += 1                    */
+#define GW_SINK_PATH_RECORD 2  /* simrank: paths[walk][visit] = v                 */
+#define GW_SINK_CLOSURE_COUNT 3/* graphlet: visits at hop >= L-1 with v == source */
+
+#define GW_MODE_RESIDENT 0 /* whole graph in HBM: one launch runs every walk out  */
+#define GW_MODE_BLOCKED 1  /* GraphWalker's block loop: supersteps over one block  */
+
+#define GW_RESIDENT_HBM 0  /* CSR copied to device memory once                   */
+#define GW_STREAM_PINNED 1 /* CSR kept in pinned host memory, blocks streamed    */
+
+/* One walk as the kernels hold it in HBM (16 bytes, one 128-bit load). */
+typedef struct gw_walk_rec {
+  uint32_t cur; /* current vertex (global id)                 */
+  uint32_t id;  /* Philox stream key (walk id)                 */
+  uint32_t src; /* source: restart target and sink key         */
+  uint32_t hop; /* hop counter                                 */
+} gw_walk_rec;
+
+typedef struct gw_walk_params {
+  uint32_t rule;        /* GW_RULE_*                                          */
+  uint32_t sink;        /* GW_SINK_*                                          */
+  uint32_t L;           /* length cap / segment length                        */
+  uint32_t njump;       /* N of `rand_r % N` (JUMP); 0 = number of vertices   */
+  double jump_prob;     /* else-branch probability; the reference's 0.15      */
+  uint64_t seed;        /* Philox key                                         */
+  uint32_t mode;        /* GW_MODE_*                                          */
+  uint32_t path_stride; /* visits recorded per walk (PATH_RECORD)             */
+  uint32_t max_hops;    /* hop guard for GW_RULE_PROB; 0 = 65535              */
+  float prob;           /* chooseBlock's min-step probability (blocked mode)  */
+  uint32_t aggregate;   /* 1 = warp-aggregate counter atomics                 */
+  uint32_t max_supersteps; /* blocked mode: stop after this many block
+                              executions, leaving the pools as they are (0 = run
+                              until no walk is pending)                        */
+  uint32_t reserved[6];
+} gw_walk_params;
+
+typedef struct gw_run_stats {
+  uint64_t walks;          /* walks run                                      */
+  uint64_t supersteps;     /* block executions (blocked mode)                */
+  uint64_t block_loads;    /* blocks copied host->device (streaming)         */
+  uint64_t bytes_h2d;      /* graph bytes copied host->device (streaming)    */
+  double ms_total;         /* device time of the last gw_run                 */
+  double ms_walk;          /* of which walk kernels                          */
+  double ms_partition;     /* of which pool partitioning                     */
+  double ms_copy_wait;     /* of which waiting for block copies              */
+} gw_run_stats;
+
+/* ---- version / codec (host only, no device needed) -------------------- */
+const char *gw_version(void);
+/* WalkManager::encode / getSourceId / getCurrentId / getHop (walk.hpp:69-84) */
+uint64_t gw_encode(uint32_t source, uint32_t current, uint32_t hop);
+uint32_t gw_get_source(uint64_t walk);
+uint32_t gw_get_current(uint64_t walk);
+uint32_t gw_get_hop(uint64_t walk);
+/* Smallest 31-bit draw r that passes `(float)r/RAND_MAX > p`
+   (randomwalkwithjump.hpp:45); the kernels compare draw >= threshold. */
+uint32_t gw_continue_threshold(double p);
+/* RandomWalk::getblock (randomwalk.hpp:74-82): nblocks when v >= blocks[nblocks] */
+uint32_t gw_getblock(const uint32_t *blocks, uint32_t nblocks, uint32_t v);
+/* compute_block (conversions.hpp:300-364): block boundaries from the row
+   pointer; returns nblocks + 1 entries written, 0 if cap is too small.     */
+uint32_t gw_compute_blocks(const uint64_t *rowptr, uint32_t nvertices, uint64_t blocksize_kb,
+                           uint32_t *blocks, uint32_t cap);
+/* RandomWalk::compBlockSize / compNmblocks (randomwalk.hpp:96-114)          */
+uint64_t gw_comp_block_size(uint64_t nwalks);
+uint32_t gw_comp_nmblocks(uint64_t blocksize_kb, uint64_t mem_budget_kb);
+
+/* ---- graph -------------------------------------------------------------- */
+typedef struct gw_graph_desc {
+  const char *base_filename; /* reads <base>_GraphWalker/graphinfo/file_0.{beg_pos,csr} */
+  uint64_t blocksize_kb;     /* and <base>_GraphWalker/blocksize_<KB>KB.blockrange     */
+  uint32_t nmblocks;         /* device block slots when streaming (0 = 2)            */
+  uint32_t residency;        /* GW_RESIDENT_HBM or GW_STREAM_PINNED                  */
+  int32_t device;            /* CUDA device ordinal                                   */
+} gw_graph_desc;
+
+/* graphwalker_engine(base, blocksize_kb, nblocks, nmblocks, m) (graphwalker.hpp:74) */
+gw_status gw_open(const gw_graph_desc *desc, gw_ctx **out);
+/* Same, from host CSR arrays (copied); blocks[nblocks+1] as in a .blockrange */
+gw_status gw_open_csr(const uint64_t *rowptr, const uint32_t *colidx, uint32_t nvertices,
+                      const uint32_t *blocks, uint32_t nblocks, uint32_t residency,
+                      int32_t device, gw_ctx **out);
+/* Seeded R-MAT graph generated on the device (self-loops dropped, duplicates
+   kept, ids permuted, rows sorted by (src, dst)); blocks from compute_block
+   with blocksize_kb.  a, b, c: quadrant probabilities (d = 1 - a - b - c).  */
+gw_status gw_open_rmat(uint32_t scale, uint32_t edge_factor, uint64_t seed, double a, double b,
+                       double c, uint64_t blocksize_kb, int32_t device, gw_ctx **out);
+gw_status gw_close(gw_ctx *ctx);
+/* Last error text of ctx (or of the calling thread when ctx is NULL). */
+const char *gw_last_error(gw_ctx *ctx);
+gw_status gw_graph_info(gw_ctx *ctx, uint32_t *nvertices, uint64_t *nedges, uint32_t *nblocks);
+gw_status gw_get_blocks(gw_ctx *ctx, uint32_t *blocks, uint32_t cap);
+/* Copies the CSR to host buffers (rowptr: nvertices+1, colidx: nedges).     */
+gw_status gw_export_csr(gw_ctx *ctx, uint64_t *rowptr, uint32_t *colidx);
+
+/* ---- walk pools (WalkManager) ------------------------------------------- */
+gw_status gw_walks_clear(gw_ctx *ctx);
+/* WalkManager::moveWalk(walk, block, t, cur) for n walks: words are the
+   reference's 64-bit walks whose current field is relative to blocks[block];
+   ids (may be NULL) key each walk's Philox stream, default = source field. */
+gw_status gw_walks_add(gw_ctx *ctx, uint32_t block, const uint64_t *words, const uint32_t *ids,
+                       size_t n);
+/* walknum[] per block and walksum (walk.hpp:25-32)                          */
+gw_status gw_walks_count(gw_ctx *ctx, uint64_t *per_block, uint64_t *total);
+
+/* ---- run ---------------------------------------------------------------- */
+/* graphwalker_engine::run(program, prob): runs every pooled walk to its end. */
+gw_status gw_run(gw_ctx *ctx, const gw_walk_params *params);
+gw_status gw_read_counts(gw_ctx *ctx, uint32_t *counts, size_t n);
+/* paths[walk * path_stride + k], lens[walk] (walks in pool order).          */
+gw_status gw_read_paths(gw_ctx *ctx, uint32_t *paths, uint32_t *lens, size_t nwalks);
+gw_status gw_read_closure(gw_ctx *ctx, uint64_t *closure);
+gw_status gw_read_stats(gw_ctx *ctx, gw_run_stats *stats);
+/* The pending walks of one block's device pool after a blocked-mode run
+   (WalkManager::getCurrentWalks, walk.hpp:114-137); *n = pool size, at most
+   cap records are copied, in pool order.                                    */
+gw_status gw_read_pool(gw_ctx *ctx, uint32_t block, gw_walk_rec *out, size_t cap, uint64_t *n);
+
+/* One call from host buffers: the walks of every pool (pool b = words
+   [pool_offsets[b], pool_offsets[b+1])) are copied in chunks that overlap
+   with the walk kernels, and the visit counts come back in counts[nvertices]
+   (VERTEX_COUNT sink; counts is overwritten).  ids may be NULL.            */
+gw_status gw_run_pools(gw_ctx *ctx, const gw_walk_params *params, const uint64_t *words,
+                       const uint64_t *pool_offsets, const uint32_t *ids, uint32_t *counts);
+
+/* ---- device-pointer entry points (stream-ordered) ----------------------- */
+/* Runs n walks resident in HBM over the whole resident graph.  Sink buffers
+   by params->sink: d_counts[nvertices] (accumulated, not cleared),
+   d_paths[n * path_stride] + d_plen[n], d_closure[1] (accumulated).        */
+gw_status gw_walk_device(gw_ctx *ctx, const gw_walk_params *params, const gw_walk_rec *d_walks,
+                         uint64_t n, uint32_t *d_counts, uint32_t *d_paths, uint32_t *d_plen,
+                         unsigned long long *d_closure, void *stream);
+/* Decodes n 64-bit walks of pool `block` into walk records (cur made global,
+   id = d_ids[i] or the source field).                                      */
+gw_status gw_unpack_words_device(gw_ctx *ctx, uint32_t block, const uint64_t *d_words,
+                                 const uint32_t *d_ids, uint64_t n, gw_walk_rec *d_out,
+                                 void *stream);
+/* Encodes walk records back to 64-bit words relative to their own block.    */
+gw_status gw_pack_words_device(gw_ctx *ctx, const gw_walk_rec *d_walks, uint64_t n,
+                               uint64_t *d_words, uint32_t *d_blocks, void *stream);
+/* Synchronises the stream and returns the device status of earlier kernels. */
+gw_status gw_sync(gw_ctx *ctx, void *stream);
+
+/* ---- measurement -------------------------------------------------------- */
+/* Random 32-byte-sector gather microbenchmark over d_buf (n_words uint32):
+   `loads` dependent-free random 4-byte loads; result in *sectors_per_s.     */
+gw_status gw_probe_gather(gw_ctx *ctx, const uint32_t *d_buf, uint64_t n_words, uint64_t loads,
+                          int iters, double *bytes_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
