@@ -59,6 +59,7 @@ def parse_args():
     ap.add_argument("--aggregate", type=int, default=0, help="warp-aggregated counter atomics")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-probe", action="store_true", help="skip the random-gather roof probe")
     ap.add_argument("--cpu-sample-sec", type=float, default=15.0)
     return ap.parse_args()
 
@@ -330,7 +331,7 @@ def our_arm(args) -> None:
 
     # random-sector gather roof: an 8 GB buffer, far larger than L2
     gather_bps = None
-    if rank == 0:
+    if rank == 0 and not args.no_probe:
         buf = torch.empty(1 << 31, dtype=torch.int32, device="cuda")
         gather_bps = G.probe_gather(buf, buf.numel(), 1 << 28, iters=5)
         del buf

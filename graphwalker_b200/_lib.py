@@ -32,7 +32,12 @@ class WalkParams(Structure):
     _fields_ = [("rule", c_uint32), ("sink", c_uint32), ("L", c_uint32), ("njump", c_uint32),
                 ("jump_prob", c_double), ("seed", c_uint64), ("mode", c_uint32),
                 ("path_stride", c_uint32), ("max_hops", c_uint32), ("prob", c_float),
-                ("aggregate", c_uint32), ("max_supersteps", c_uint32), ("reserved", c_uint32 * 6)]
+                ("aggregate", c_uint32), ("max_supersteps", c_uint32), ("cache_hints", c_uint32),
+                ("reserved", c_uint32 * 5)]
+
+
+HINT_EXPLICIT = 0x80000000
+HINT_COLUMNS_EVICT_FIRST, HINT_COUNTS_EVICT_LAST, HINT_RECORDS_EVICT_LAST = 1, 2, 4
 
 
 class RunStats(Structure):
@@ -88,6 +93,8 @@ _SIGS = {
     "gw_pack_words_device": (c_int32, [_P, _P, c_uint64, _P, _P, _P]),
     "gw_sync": (c_int32, [_P, _P]),
     "gw_probe_gather": (c_int32, [_P, _P, c_uint64, c_uint64, ctypes.c_int, POINTER(c_double)]),
+    "gw_set_l2_fetch_granularity": (c_int32, [_P, c_uint32, POINTER(c_uint32)]),
+    "gw_set_l2_persisting": (c_int32, [_P, c_uint64]),
 }
 
 _lib = None

@@ -113,6 +113,15 @@ gw_status install_graph(gw_ctx* ctx, const uint64_t* rowptr, const uint32_t* col
   return GW_OK;
 }
 
+// By default a context reserves L2 for its visit counters (persisting access
+// policy window, see gw_set_l2_persisting); GW_L2_PERSIST=0 disables it.
+void default_l2_persisting(gw_ctx* ctx) {
+  const char* env = getenv("GW_L2_PERSIST");
+  if (env && strcmp(env, "0") == 0) return;
+  gw_set_l2_persisting(ctx, (uint64_t)ctx->nv * sizeof(uint32_t));
+  ctx->err.clear();  // a device without persisting L2 simply runs without it
+}
+
 uint32_t prob_to_u32(double x) {
   if (x <= 0.0) return 0;
   const double v = std::floor(x * 4294967296.0 + 0.5);
@@ -133,6 +142,7 @@ gw_status make_walk_args(gw_ctx* ctx, const gw_walk_params* p, WalkArgs* a) {
     return ctx->fail(GW_E_INVALID, "PATH_RECORD needs path_stride >= 1");
   if (!(p->jump_prob >= 0.0 && p->jump_prob <= 1.0))
     return ctx->fail(GW_E_INVALID, "jump_prob must lie in [0, 1]");
+  a->hints = (p->cache_hints & GW_HINT_EXPLICIT) ? (p->cache_hints & 7u) : kDefaultHints;
   a->L = p->L;
   a->thr = gw_continue_threshold(p->jump_prob);
   a->njump = p->njump ? p->njump : ctx->nv;
@@ -293,6 +303,7 @@ gw_status gw_open(const gw_graph_desc* desc, gw_ctx** out) {
     gw_close(ctx);
     return s;
   }
+  default_l2_persisting(ctx);
   *out = ctx;
   return GW_OK;
 }
@@ -314,6 +325,7 @@ gw_status gw_open_csr(const uint64_t* rowptr, const uint32_t* colidx, uint32_t n
     gw_close(ctx);
     return s;
   }
+  default_l2_persisting(ctx);
   *out = ctx;
   return GW_OK;
 }
@@ -371,6 +383,7 @@ gw_status gw_open_rmat(uint32_t scale, uint32_t edge_factor, uint64_t seed, doub
     gw_close(ctx);
     return s;
   }
+  default_l2_persisting(ctx);
   *out = ctx;
   return GW_OK;
 }
@@ -379,6 +392,7 @@ gw_status gw_close(gw_ctx* ctx) {
   if (!ctx) return GW_OK;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+  if (ctx->l2_persist_bytes) gw_set_l2_persisting(ctx, 0);
   for (gw_devbuf* b : {&ctx->d_rowptr, &ctx->d_colidx, &ctx->d_vrec, &ctx->d_blocks, &ctx->d_status,
                        &ctx->d_walks, &ctx->d_words, &ctx->d_ids, &ctx->d_counts, &ctx->d_paths,
                        &ctx->d_plen, &ctx->d_closure, &ctx->d_pool_offsets, &ctx->d_dest,
@@ -522,9 +536,11 @@ gw_status gw_run(gw_ctx* ctx, const gw_walk_params* params) {
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, st);
+  cudaAccessPolicyWindow win;
+  const bool use_win = params->sink == GW_SINK_VERTEX_COUNT && ctx->counts_window(sv.counts, &win);
   cudaError_t e = gw::launch_walk_resident((int)params->rule, (int)params->sink, params->aggregate != 0,
                                            ctx->d_walks.as<gw_walk_rec>(), n, ctx->view(), a, sv,
-                                           ctx->d_status.as<uint32_t>(), 0, st);
+                                           ctx->d_status.as<uint32_t>(), 0, st, use_win ? &win : nullptr);
   cudaEventRecord(e1, st);
   if (e != cudaSuccess) {
     cudaEventDestroy(e0);
@@ -640,10 +656,12 @@ gw_status gw_run_pools(gw_ctx* ctx, const gw_walk_params* params, const uint64_t
                                   ids ? ctx->d_ids.as<uint32_t>() + lo : nullptr, lo, m,
                                   ctx->d_pool_offsets.as<uint64_t>(), ctx->d_blocks.as<uint32_t>(),
                                   ctx->nblocks, ctx->d_walks.as<gw_walk_rec>() + lo, cs);
+    cudaAccessPolicyWindow win;
+    const bool use_win = params->sink == GW_SINK_VERTEX_COUNT && ctx->counts_window(sv.counts, &win);
     if (e == cudaSuccess)
       e = gw::launch_walk_resident((int)params->rule, (int)params->sink, params->aggregate != 0,
                                    ctx->d_walks.as<gw_walk_rec>() + lo, m, ctx->view(), a, sv,
-                                   ctx->d_status.as<uint32_t>(), 0, cs);
+                                   ctx->d_status.as<uint32_t>(), 0, cs, use_win ? &win : nullptr);
   }
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(counts, ctx->d_counts.p, (size_t)ctx->nv * 4, cudaMemcpyDeviceToHost, cs);
@@ -677,11 +695,39 @@ gw_status gw_walk_device(gw_ctx* ctx, const gw_walk_params* params, const gw_wal
   if (params->sink == GW_SINK_PATH_RECORD && (!d_paths || !d_plen))
     return ctx->fail(GW_E_INVALID, "d_paths/d_plen is NULL");
   if (params->sink == GW_SINK_CLOSURE_COUNT && !d_closure) return ctx->fail(GW_E_INVALID, "d_closure is NULL");
-  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  cudaStream_t st = (cudaStream_t)stream;  // NULL = the default stream
+  cudaAccessPolicyWindow win;
+  const bool use_win = params->sink == GW_SINK_VERTEX_COUNT && ctx->counts_window(d_counts, &win);
   cudaError_t e = gw::launch_walk_resident((int)params->rule, (int)params->sink, params->aggregate != 0,
                                            d_walks, n, ctx->view(), a, sv,
-                                           ctx->d_status.as<uint32_t>(), 0, st);
+                                           ctx->d_status.as<uint32_t>(), 0, st, use_win ? &win : nullptr);
   if (e != cudaSuccess) return ctx->cuda_fail(e, "walk kernel launch");
+  return GW_OK;
+}
+
+gw_status gw_set_l2_fetch_granularity(gw_ctx* ctx, uint32_t bytes, uint32_t* previous) {
+  if (!ctx) return set_thread_error(GW_E_INVALID, "NULL context");
+  size_t old = 0;
+  GW_CUDA(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  GW_CUDA(ctx, cudaDeviceGetLimit(&old, cudaLimitMaxL2FetchGranularity), "get L2 fetch granularity");
+  if (previous) *previous = (uint32_t)old;
+  if (bytes) {
+    if (bytes > 128 || (bytes & (bytes - 1))) return ctx->fail(GW_E_INVALID, "granularity must be a power of two <= 128");
+    GW_CUDA(ctx, cudaDeviceSetLimit(cudaLimitMaxL2FetchGranularity, bytes), "set L2 fetch granularity");
+  }
+  return GW_OK;
+}
+
+gw_status gw_set_l2_persisting(gw_ctx* ctx, uint64_t bytes) {
+  if (!ctx) return set_thread_error(GW_E_INVALID, "NULL context");
+  GW_CUDA(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  int max_persist = 0;
+  GW_CUDA(ctx, cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, ctx->device),
+          "max persisting L2");
+  const uint64_t b = std::min<uint64_t>(bytes, (uint64_t)max_persist);
+  GW_CUDA(ctx, cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, (size_t)b), "persisting L2 limit");
+  if (b == 0) GW_CUDA(ctx, cudaCtxResetPersistingL2Cache(), "reset persisting L2");
+  ctx->l2_persist_bytes = b;
   return GW_OK;
 }
 
@@ -690,7 +736,7 @@ gw_status gw_unpack_words_device(gw_ctx* ctx, uint32_t block, const uint64_t* d_
                                  void* stream) {
   if (!ctx) return set_thread_error(GW_E_INVALID, "NULL context");
   if (block >= ctx->nblocks) return ctx->fail(GW_E_INVALID, "block %u >= nblocks", block);
-  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  cudaStream_t st = (cudaStream_t)stream;  // NULL = the default stream
   GW_CUDA(ctx, gw::launch_unpack_words(d_words, d_ids, n, ctx->blocks[block], d_out, st), "unpack");
   return GW_OK;
 }
@@ -698,7 +744,7 @@ gw_status gw_unpack_words_device(gw_ctx* ctx, uint32_t block, const uint64_t* d_
 gw_status gw_pack_words_device(gw_ctx* ctx, const gw_walk_rec* d_walks, uint64_t n,
                                uint64_t* d_words, uint32_t* d_blocks, void* stream) {
   if (!ctx) return set_thread_error(GW_E_INVALID, "NULL context");
-  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  cudaStream_t st = (cudaStream_t)stream;  // NULL = the default stream
   GW_CUDA(ctx, gw::launch_pack_words(d_walks, n, ctx->d_blocks.as<uint32_t>(), ctx->nblocks, d_words,
                                      d_blocks, st), "pack");
   return GW_OK;
@@ -706,7 +752,7 @@ gw_status gw_pack_words_device(gw_ctx* ctx, const gw_walk_rec* d_walks, uint64_t
 
 gw_status gw_sync(gw_ctx* ctx, void* stream) {
   if (!ctx) return set_thread_error(GW_E_INVALID, "NULL context");
-  return gw::take_status(ctx, stream ? (cudaStream_t)stream : ctx->stream);
+  return gw::take_status(ctx, (cudaStream_t)stream);
 }
 
 gw_status gw_probe_gather(gw_ctx* ctx, const uint32_t* d_buf, uint64_t n_words, uint64_t loads,

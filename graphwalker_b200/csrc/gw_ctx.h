@@ -95,7 +95,22 @@ struct gw_ctx {
   std::vector<uint64_t> pool_size;
   std::vector<uint32_t> minstep;  // per-block min hop (WalkManager::minstep)
 
+  // L2 persisting reservation for the visit counters (0 = none)
+  uint64_t l2_persist_bytes = 0;
+
   std::string err;
+
+  // Access policy window over `counts` when an L2 reservation is active.
+  bool counts_window(const void* counts, cudaAccessPolicyWindow* w) const {
+    if (!l2_persist_bytes || !counts) return false;
+    const size_t bytes = (size_t)nv * sizeof(uint32_t);
+    w->base_ptr = const_cast<void*>(counts);
+    w->num_bytes = bytes;
+    w->hitRatio = bytes <= l2_persist_bytes ? 1.0f : (float)l2_persist_bytes / (float)bytes;
+    w->hitProp = cudaAccessPropertyPersisting;
+    w->missProp = cudaAccessPropertyStreaming;
+    return true;
+  }
 
   gw_status fail(gw_status code, const char* fmt, ...) {
     char buf[512];

@@ -50,9 +50,44 @@ __host__ __device__ __forceinline__ Philox4 philox4x32_10(uint32_t c0, uint32_t 
   return Philox4{c0, c1, c2, c3};
 }
 
+// ---- L2 eviction-priority hints (PTX createpolicy / .L2::cache_hint) ----
+// The column array is read once per visit at a random position and gains
+// nothing from staying in L2; the visit counters are read-modify-written at
+// every visit and the vertex records of hub vertices are re-read often.
+// Hints let the kernel keep the latter resident at the expense of the former.
+constexpr uint32_t kHintColumnsEvictFirst = 1u;
+constexpr uint32_t kHintCountsEvictLast = 2u;
+constexpr uint32_t kHintRecordsEvictLast = 4u;
+
+__device__ __forceinline__ uint64_t l2_policy(bool first, bool last) {
+  uint64_t p;
+  if (first) asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  else if (last) asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  else asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ uint32_t ld_nc_u32(const uint32_t* a, uint64_t pol) {
+  uint32_t r;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(r) : "l"(a), "l"(pol));
+  return r;
+}
+
+__device__ __forceinline__ unsigned long long ld_nc_u64(const unsigned long long* a, uint64_t pol) {
+  unsigned long long r;
+  asm volatile("ld.global.nc.L2::cache_hint.b64 %0, [%1], %2;" : "=l"(r) : "l"(a), "l"(pol));
+  return r;
+}
+
+__device__ __forceinline__ void red_add_u32(uint32_t* a, uint32_t v, uint64_t pol) {
+  asm volatile("red.relaxed.gpu.global.add.L2::cache_hint.u32 [%0], %1, %2;" ::"l"(a), "r"(v), "l"(pol)
+               : "memory");
+}
+
 // Launch-constant parameters of a walk kernel (passed by value, lands in the
 // constant bank).
 struct WalkArgs {
+  uint32_t hints;      // kHint* bits
   uint32_t L;          // length cap (JUMP/STOP/PPR) or segment length (RESTART)
   uint32_t thr;        // continuation passes iff draw >= thr
   uint32_t njump;      // JUMP target range
@@ -84,10 +119,22 @@ __device__ __forceinline__ constexpr bool rule_capped() {
 // One hop of one walk at vertex v (already visited).  Returns false when the
 // walk ends inside this hop (stop rules); otherwise v is the next vertex and
 // the caller increments the hop.  Loads go through the read-only path.
+struct L2Hints {
+  uint64_t rec, col, cnt;
+};
+
+__device__ __forceinline__ L2Hints make_hints(uint32_t flags) {
+  L2Hints h;
+  h.rec = l2_policy(false, flags & kHintRecordsEvictLast);
+  h.col = l2_policy(flags & kHintColumnsEvictFirst, false);
+  h.cnt = l2_policy(false, flags & kHintCountsEvictLast);
+  return h;
+}
+
 template <int RULE>
-__device__ __forceinline__ bool hop_advance(const GraphView& g, const WalkArgs& a, uint32_t id,
-                                            uint32_t src, uint32_t hop, uint32_t& v) {
-  const unsigned long long rec = __ldg(g.vrec + v);
+__device__ __forceinline__ bool hop_advance(const GraphView& g, const WalkArgs& a, const L2Hints& hp,
+                                            uint32_t id, uint32_t src, uint32_t hop, uint32_t& v) {
+  const unsigned long long rec = ld_nc_u64(g.vrec + v, hp.rec);
   const Philox4 ph = philox4x32_10(id, hop, 0u, 0u, a.seed_lo, a.seed_hi);
   const uint32_t d0 = ph.x >> 1;
   const uint32_t d1 = ph.y >> 1;
@@ -102,7 +149,7 @@ __device__ __forceinline__ bool hop_advance(const GraphView& g, const WalkArgs& 
     // (eid_t)rand_r % outd with a 31-bit draw: equals the draw when outd > 2^31
     const unsigned long long r =
         deg > 0x7fffffffull ? (unsigned long long)d1 : (unsigned long long)(d1 % (uint32_t)deg);
-    v = __ldg(g.colidx + off + r);
+    v = ld_nc_u32(g.colidx + off + r, hp.col);
     return true;
   }
   const uint32_t dj = deg > 0 ? d1 : d0;
@@ -165,14 +212,14 @@ __device__ __forceinline__ bool hop_advance_slice(const unsigned long long* __re
 // vertex in the same instruction into one atomic (hub vertices, and every
 // walk of a single-source query at hop 0).
 template <bool AGG>
-__device__ __forceinline__ void count_visit(uint32_t* __restrict__ counts, uint32_t v) {
+__device__ __forceinline__ void count_visit(uint32_t* __restrict__ counts, uint32_t v, uint64_t pol) {
   if (AGG) {
     const unsigned active = __activemask();
     const unsigned peers = __match_any_sync(active, v);
     const int lane = threadIdx.x & 31;
-    if (lane == __ffs(peers) - 1) atomicAdd(counts + v, (uint32_t)__popc(peers));
+    if (lane == __ffs(peers) - 1) red_add_u32(counts + v, (uint32_t)__popc(peers), pol);
   } else {
-    atomicAdd(counts + v, 1u);
+    red_add_u32(counts + v, 1u, pol);
   }
 }
 

@@ -30,6 +30,7 @@ __global__ void __launch_bounds__(kWalkThreads)
   uint32_t v = w.x, id = w.y, src = w.z, hop = w.w, k = 0;
   uint32_t st = 0;
   uint32_t clos = 0;
+  const L2Hints hp = make_hints(a.hints);
   for (;;) {
     bool end;
     if (rule_capped<RULE>() && hop >= a.L) {
@@ -43,7 +44,7 @@ __global__ void __launch_bounds__(kWalkThreads)
     } else {
       // the app's updateInfo(src, v, tid, hop) precedes the draws
       if (SINK == GW_SINK_VERTEX_COUNT) {
-        count_visit<AGG>(s.counts, v);
+        count_visit<AGG>(s.counts, v, hp.cnt);
       } else if (SINK == GW_SINK_PATH_RECORD) {
         if (k < a.path_stride) s.paths[i * a.path_stride + k] = v;
         else st |= kStOverflow;
@@ -51,7 +52,7 @@ __global__ void __launch_bounds__(kWalkThreads)
         clos += ((int)hop >= (int)a.L - 1 && v == src) ? 1u : 0u;
       }
       ++k;
-      end = !hop_advance<RULE>(g, a, id, src, hop, v);
+      end = !hop_advance<RULE>(g, a, hp, id, src, hop, v);
       if (!end) {
         ++hop;
         if (RULE == GW_RULE_RESTART && hop % a.L == a.L - 1) end = true;
@@ -97,6 +98,7 @@ __global__ void __launch_bounds__(kWalkThreads)
                       uint32_t* __restrict__ dest, uint32_t* __restrict__ status) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   uint32_t st = 0, clos = 0;
+  const L2Hints hp = make_hints(a.hints);
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     uint4 w = *(reinterpret_cast<const uint4*>(walks) + i);
     uint32_t v = w.x, id = w.y, src = w.z, hop = w.w;
@@ -113,12 +115,12 @@ __global__ void __launch_bounds__(kWalkThreads)
         ended = true;
         break;
       }
-      if (SINK == GW_SINK_VERTEX_COUNT) count_visit<AGG>(s.counts, v);
+      if (SINK == GW_SINK_VERTEX_COUNT) count_visit<AGG>(s.counts, v, hp.cnt);
       else if (SINK == GW_SINK_CLOSURE_COUNT)
         clos += ((int)hop >= (int)a.L - 1 && v == src) ? 1u : 0u;
       bool moved;
       if (SLICE) moved = hop_advance_slice<RULE>(beg_pos, csr, a, id, src, hop, v);
-      else moved = hop_advance<RULE>(g, a, id, src, hop, v);
+      else moved = hop_advance<RULE>(g, a, hp, id, src, hop, v);
       if (!moved) {
         ended = true;
         break;
@@ -210,17 +212,20 @@ __global__ void __launch_bounds__(256)
                         unsigned long long* __restrict__ sink) {
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   uint32_t acc = 0;
-  const uint64_t nsect = n_words / 8;
+  // sectors in the buffer, rounded down to a power of two (mask, no modulo)
+  uint64_t nsect = 1;
+  while (nsect * 2 <= n_words / 8) nsect *= 2;
+  const uint32_t mask = (uint32_t)(nsect - 1);
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < loads; i += stride * 4) {
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const uint64_t j = i + u * stride;
       if (j < loads) {
-        uint64_t h = j * 0x9E3779B97F4A7C15ull;
-        h ^= h >> 29;
-        h *= 0xBF58476D1CE4E5B9ull;
-        h ^= h >> 32;
-        acc += __ldg(buf + (h % nsect) * 8 + (j & 7));
+        uint32_t h = (uint32_t)j * 0x9E3779B9u;
+        h ^= h >> 15;
+        h *= 0x85EBCA6Bu;
+        h ^= h >> 13;
+        acc += __ldg(buf + (uint64_t)(h & mask) * 8 + (j & 7));
       }
     }
   }
@@ -252,11 +257,23 @@ int occupancy_grid(K kernel, uint64_t n) {
 template <int RULE, int SINK, bool AGG>
 cudaError_t resident_dispatch(const gw_walk_rec* walks, uint64_t n, const GraphView& g,
                               const WalkArgs& a, const SinkView& s, uint32_t* status, int grid,
-                              cudaStream_t stream) {
+                              cudaStream_t stream, const cudaAccessPolicyWindow* window) {
   auto k = walk_resident_kernel<RULE, SINK, AGG>;
   if (grid <= 0) grid = occupancy_grid(k, n);
-  k<<<grid, kWalkThreads, 0, stream>>>(walks, n, g, a, s, status);
-  return cudaGetLastError();
+  if (!window) {
+    k<<<grid, kWalkThreads, 0, stream>>>(walks, n, g, a, s, status);
+    return cudaGetLastError();
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kWalkThreads);
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
+  attr[0].val.accessPolicyWindow = *window;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, walks, n, g, a, s, status);
 }
 
 template <int RULE, int SINK, bool AGG>
@@ -305,9 +322,10 @@ cudaError_t block_dispatch(gw_walk_rec* walks, uint64_t n, const GraphView& g,
 
 cudaError_t launch_walk_resident(int rule, int sink, bool agg, const gw_walk_rec* walks, uint64_t n,
                                  const GraphView& g, const WalkArgs& a, const SinkView& s,
-                                 uint32_t* status, int grid, cudaStream_t stream) {
+                                 uint32_t* status, int grid, cudaStream_t stream,
+                                 const cudaAccessPolicyWindow* window) {
   if (n == 0) return cudaSuccess;
-  GW_RULE_CASES(resident_dispatch, walks, n, g, a, s, status, grid, stream)
+  GW_RULE_CASES(resident_dispatch, walks, n, g, a, s, status, grid, stream, window)
   return cudaErrorInvalidValue;
 }
 

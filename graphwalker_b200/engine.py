@@ -33,13 +33,15 @@ def _ptr(a) -> int | None:
 def params(rule: int = RULE_JUMP, sink: int = SINK_VERTEX_COUNT, L: int = 10, *, njump: int = 0,
            jump_prob: float = 0.15, seed: int = 42, mode: int = MODE_RESIDENT, path_stride: int = 0,
            max_hops: int = 0, prob: float = 0.2, aggregate: bool = False,
-           max_supersteps: int = 0) -> WalkParams:
-    """gw_walk_params with the reference's defaults (0.15 else-branch, prob 0.2)."""
+           max_supersteps: int = 0, cache_hints: int | None = None) -> WalkParams:
+    """gw_walk_params with the reference's defaults (0.15 else-branch, prob 0.2).
+    cache_hints: None = engine default, else GW_HINT_* bits used as given."""
     p = WalkParams()
     p.rule, p.sink, p.L, p.njump = rule, sink, L, njump
     p.jump_prob, p.seed, p.mode = jump_prob, seed & 0xFFFFFFFFFFFFFFFF, mode
     p.path_stride, p.max_hops, p.prob, p.aggregate = path_stride, max_hops, prob, int(aggregate)
     p.max_supersteps = max_supersteps
+    p.cache_hints = 0 if cache_hints is None else (_lib.HINT_EXPLICIT | cache_hints)
     return p
 
 
@@ -226,6 +228,15 @@ class Graph:
 
     def sync(self, stream: int | None = None) -> None:
         check(load().gw_sync(self._h, stream), self._h)
+
+    def set_l2_fetch_granularity(self, nbytes: int) -> int:
+        """Sets the context's L2 fetch granularity (0 = leave); returns the old one."""
+        old = c_uint32()
+        check(load().gw_set_l2_fetch_granularity(self._h, nbytes, byref(old)), self._h)
+        return old.value
+
+    def set_l2_persisting(self, nbytes: int) -> None:
+        check(load().gw_set_l2_persisting(self._h, nbytes), self._h)
 
     def probe_gather(self, buf, n_words: int, loads: int, iters: int = 5) -> float:
         out = c_double()

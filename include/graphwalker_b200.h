@@ -9,7 +9,7 @@
  * Ownership: a gw_ctx owns every device buffer it allocates; the caller owns
  * every host buffer it passes, and no pointer is retained past the call that
  * received it.  *_device entry points take device pointers and a CUDA
- * stream (cudaStream_t passed as void*, NULL = the context's stream) and are
+ * stream (cudaStream_t passed as void*; NULL = the default stream) and are
  * stream-ordered: they return once the work is enqueued.
  * Errors: every call returns a gw_status (0 = GW_OK).  Device-side
  * violations (an out-of-range vertex id, a full sink) are reported through a
@@ -65,6 +65,11 @@ typedef struct gw_ctx gw_ctx;
 #define GW_MODE_RESIDENT 0 /* whole graph in HBM: one launch runs every walk out  */
 #define GW_MODE_BLOCKED 1  /* GraphWalker's block loop: supersteps over one block  */
 
+#define GW_HINT_EXPLICIT 0x80000000u    /* cache_hints: use exactly these bits     */
+#define GW_HINT_COLUMNS_EVICT_FIRST 1u  /* column loads leave L2 first              */
+#define GW_HINT_COUNTS_EVICT_LAST 2u    /* visit-counter atomics stay in L2         */
+#define GW_HINT_RECORDS_EVICT_LAST 4u   /* vertex-record loads stay in L2           */
+
 #define GW_RESIDENT_HBM 0  /* CSR copied to device memory once                   */
 #define GW_STREAM_PINNED 1 /* CSR kept in pinned host memory, blocks streamed    */
 
@@ -91,7 +96,9 @@ typedef struct gw_walk_params {
   uint32_t max_supersteps; /* blocked mode: stop after this many block
                               executions, leaving the pools as they are (0 = run
                               until no walk is pending)                        */
-  uint32_t reserved[6];
+  uint32_t cache_hints; /* L2 eviction priorities of the walk kernels: 0 = the
+                           engine default; otherwise GW_HINT_EXPLICIT | bits  */
+  uint32_t reserved[5];
 } gw_walk_params;
 
 typedef struct gw_run_stats {
@@ -200,6 +207,16 @@ gw_status gw_pack_words_device(gw_ctx *ctx, const gw_walk_rec *d_walks, uint64_t
                                uint64_t *d_words, uint32_t *d_blocks, void *stream);
 /* Synchronises the stream and returns the device status of earlier kernels. */
 gw_status gw_sync(gw_ctx *ctx, void *stream);
+
+/* ---- L2 controls (per CUDA context; nothing outlasts the process) ------- */
+/* cudaLimitMaxL2FetchGranularity for this process's context: the bytes L2
+   fetches from DRAM on a miss (32 suits random 4/8-byte gathers).  0 leaves
+   the limit unchanged; *previous (may be NULL) receives the old value.     */
+gw_status gw_set_l2_fetch_granularity(gw_ctx *ctx, uint32_t bytes, uint32_t *previous);
+/* Reserves up to `bytes` of L2 for persisting accesses and marks the visit
+   counters of later VERTEX_COUNT walk launches as persisting (an access
+   policy window on the launch).  0 releases the reservation.               */
+gw_status gw_set_l2_persisting(gw_ctx *ctx, uint64_t bytes);
 
 /* ---- measurement -------------------------------------------------------- */
 /* Random 32-byte-sector gather microbenchmark over d_buf (n_words uint32):

@@ -65,6 +65,16 @@ int gwo_continue_test(uint32_t r, double p) {
     return (double)q > p;
 }
 
+uint64_t gwo_threshold_mismatches(double p) {
+    uint32_t thr = gwo_continue_threshold(p);
+    uint64_t bad = 0;
+    for (uint32_t r = 0; r < 0x80000000u; ++r) {
+        float q = (float)(int)r / GWO_RAND_MAX;
+        bad += ((double)q > p) != (r >= thr);
+    }
+    return bad;
+}
+
 uint32_t gwo_continue_threshold(double p) {
     uint32_t lo = 0, hi = 0x80000000u; /* answer in [lo, hi] */
     if (!gwo_continue_test(0x7fffffffu, p)) return 0x80000000u;

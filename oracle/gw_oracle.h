@@ -55,6 +55,10 @@ uint32_t gwo_continue_threshold(double p);
  * the reference's `(float)rand_r(&seed)/RAND_MAX > 0.15` does. */
 int gwo_continue_test(uint32_t r, double p);
 
+/* Number of r in [0, 2^31) where `r >= gwo_continue_threshold(p)` disagrees
+ * with the float test (exhaustive; 0 expected). */
+uint64_t gwo_threshold_mismatches(double p);
+
 /* The reference's 64-bit walk word (src/walks/walk.hpp:69-91). */
 uint64_t gwo_encode(uint32_t source, uint32_t current, uint32_t hop);
 uint32_t gwo_get_source(uint64_t w);

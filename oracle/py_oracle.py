@@ -51,6 +51,7 @@ def lib() -> ctypes.CDLL:
             "gwo_philox4x32_10": (None, [P, P, P]),
             "gwo_continue_threshold": (c_uint32, [c_double]),
             "gwo_continue_test": (ctypes.c_int, [c_uint32, c_double]),
+            "gwo_threshold_mismatches": (c_uint64, [c_double]),
             "gwo_encode": (c_uint64, [c_uint32, c_uint32, c_uint32]),
             "gwo_get_source": (c_uint32, [c_uint64]),
             "gwo_get_current": (c_uint32, [c_uint64]),

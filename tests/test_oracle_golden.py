@@ -32,6 +32,12 @@ def test_continue_threshold_matches_float_test(oracle):
     assert oracle.continue_threshold(1.0) == 2**31
 
 
+def test_continue_threshold_exhaustive(oracle):
+    # every 31-bit draw: the integer comparison the kernels make equals the
+    # reference's float expression for the reference's 0.15
+    assert oracle.lib().gwo_threshold_mismatches(0.15) == 0
+
+
 def test_codec_matches_walk_hpp(oracle):
     lib = oracle.lib()
     rng = np.random.default_rng(5)
