@@ -93,6 +93,7 @@ _SIGS = {
     "gw_pack_words_device": (c_int32, [_P, _P, c_uint64, _P, _P, _P]),
     "gw_sync": (c_int32, [_P, _P]),
     "gw_probe_gather": (c_int32, [_P, _P, c_uint64, c_uint64, ctypes.c_int, POINTER(c_double)]),
+    "gw_superstep_static": (c_int32, [_P, POINTER(WalkParams), c_uint32, _P, c_uint64, _P, _P, _P, _P, _P]),
     "gw_set_l2_fetch_granularity": (c_int32, [_P, c_uint32, POINTER(c_uint32)]),
     "gw_set_l2_persisting": (c_int32, [_P, c_uint64]),
 }

@@ -208,6 +208,28 @@ gw_status gw_pack_words_device(gw_ctx *ctx, const gw_walk_rec *d_walks, uint64_t
 /* Synchronises the stream and returns the device status of earlier kernels. */
 gw_status gw_sync(gw_ctx *ctx, void *stream);
 
+/* One superstep of the blocked engine that allocates no memory.  This entry
+   point has no counterpart in the reference (whose engine allocates host
+   buffers per block); it exists for callers that cannot call cudaMalloc
+   while they drive walks: a host framework whose caching allocator already
+   holds the device's free memory, or a serving loop that must not stall on
+   the device-wide synchronisation an allocation or free can cause.
+   The n walks of `block` (d_walks, device records) are advanced while they
+   stay inside the block (in place, as gw_run's blocked mode does); visits go
+   to d_counts (VERTEX_COUNT sink, accumulated); the walks that left the block
+   are written to d_moved grouped by destination block, each group in input
+   order, group d starting at d_offsets[d] (nblocks + 1 entries, the last =
+   walks moved); d_minhop[d] = lowest hop moved into block d (0xffffffff if
+   none).  All scratch comes from one fixed device array of the library
+   (about 12 MiB per GPU that loads it, held until exit): at most 1,048,576
+   walks and 256 blocks per call, else GW_E_INVALID.  The first call on a
+   device looks up that array's address, so make it before any stream
+   capture.  Calls share the array: two calls that overlap on the GPU race. */
+gw_status gw_superstep_static(gw_ctx *ctx, const gw_walk_params *params, uint32_t block,
+                              gw_walk_rec *d_walks, uint64_t n, uint32_t *d_counts,
+                              gw_walk_rec *d_moved, uint32_t *d_offsets, uint32_t *d_minhop,
+                              void *stream);
+
 /* ---- L2 controls (per CUDA context; nothing outlasts the process) ------- */
 /* cudaLimitMaxL2FetchGranularity for this process's context: the bytes L2
    fetches from DRAM on a miss (32 suits random 4/8-byte gathers).  0 leaves
