@@ -1,0 +1,141 @@
+"""The drop-in C++ API (graphwalker_b200/compat): GraphWalker programs compile
+unchanged against it, and a program written against GraphWalker's API,
+running on the B200 engine, receives in its updateInfo exactly the visits
+the reference engine delivers (golden vectors, Philox-keyed draws)."""
+import os
+import re
+import struct
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, golden_runs, load_golden
+
+COMPAT = ROOT / "graphwalker_b200" / "compat"
+APPS_DIR = COMPAT / "_apps"
+REFERENCE_APPS = Path("/root/reference/apps")
+LIVE_APPS = ["rwdomination", "rawrandomwalks", "msppr", "kk_ppr", "graphlet", "simrank"]
+
+
+def build_compat_app(rule: int, out: Path) -> Path:
+    subprocess.run(["make", "-s", "-C", str(COMPAT), "app", f"SRC={ROOT / 'tests' / 'compat' / 'gw_compat_app.cpp'}",
+                    f"OUT={out}", f"DEFS=-DGW_APP_RULE={rule}"], check=True)
+    return out
+
+
+@pytest.mark.skipif(not REFERENCE_APPS.is_dir(), reason="needs the reference's apps/ sources")
+def test_reference_apps_compile_unchanged():
+    subprocess.run(["make", "-s", "-C", str(COMPAT), "apps", f"REF={REFERENCE_APPS.parent}"], check=True)
+    for app in LIVE_APPS:
+        assert (APPS_DIR / app).exists(), app
+
+
+def test_compat_program_compiles(tmp_path):
+    for rule in range(4):
+        assert build_compat_app(rule, tmp_path / f"app{rule}").exists()
+
+
+def _prepare(tmp: Path, g: dict, name: str) -> str:
+    from graphwalker_b200 import formats
+    (tmp / "conf").mkdir(exist_ok=True)
+    (tmp / "conf" / "graphwalker.cnf").write_text("# empty\n")
+    base = str(tmp / name)
+    formats.write_graph(base, g["rowptr"], g["colidx"], int(g["blocksize_kb"]))
+    return base
+
+
+def _walks_file(path: Path, g: dict, tag: str):
+    import graphwalker_b200 as gw
+    cur, src, hop = g[f"{tag}_cur"], g[f"{tag}_src"], g[f"{tag}_hop"]
+    blocks = g["blocks"]
+    blk = np.searchsorted(blocks[1:], cur, side="right").astype(np.uint32)
+    rec = np.zeros(len(cur), dtype=[("b", "<u4"), ("pad", "<u4"), ("w", "<u8")])
+    rec["b"] = blk
+    rec["w"] = gw.encode(src, cur - blocks[blk], hop)
+    with open(path, "wb") as f:
+        f.write(struct.pack("<Q", len(cur)))
+        f.write(rec.tobytes())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["hand", "rmat10", "rmat13"])
+def test_compat_program_matches_reference_goldens(cuda_device, case, tmp_path):
+    g = load_golden(case)
+    base = _prepare(tmp_path, g, case)
+    nv = len(g["rowptr"]) - 1
+    bins = {}
+    for tag in golden_runs(g):
+        rule, L = int(g[f"{tag}_rule"]), int(g[f"{tag}_L"])
+        if rule not in bins:
+            bins[rule] = build_compat_app(rule, tmp_path / f"app{rule}")
+        gp = g[f"{tag}_paths"]
+        nkeys, stride = gp.shape
+        _walks_file(tmp_path / "walks.bin", g, tag)
+        out = tmp_path / "out.bin"
+        subprocess.run([str(bins[rule]), base, str(int(g["blocksize_kb"])), str(tmp_path / "walks.bin"), str(out),
+                        str(L), str(int(g["seed"])), str(nv), str(nkeys), str(stride),
+                        "gw_walk_id", "source", "seed", str(int(g["seed"]))],
+                       cwd=tmp_path, check=True, capture_output=True)
+        raw = out.read_bytes()
+        counts = np.frombuffer(raw, np.uint32, nv, 8)
+        paths = np.frombuffer(raw, np.uint32, nkeys * stride, 8 + 4 * nv).reshape(nkeys, stride)
+        closure = struct.unpack_from("<Q", raw, 8 + 4 * nv + 4 * nkeys * stride)[0]
+        assert np.array_equal(counts, g[f"{tag}_counts"]), f"{case}/{tag}"
+        assert np.array_equal(paths, gp), f"{case}/{tag} paths"
+        assert closure == int(g[f"{tag}_closure"])
+
+
+def _run_app(app: str, args: list[str], cwd: Path) -> subprocess.CompletedProcess:
+    exe = APPS_DIR / app
+    if not exe.exists():
+        pytest.skip(f"{exe} not built (make -C graphwalker_b200/compat apps)")
+    return subprocess.run([str(exe), *args], cwd=cwd, capture_output=True, text=True, timeout=300)
+
+
+@pytest.mark.gpu
+def test_unchanged_simrank_app(cuda_device, tmp_path):
+    """apps/simrank.cpp, unchanged, on the B200 engine: its SimRank equals the
+    value computed from the reference engine's golden walk paths."""
+    g = load_golden("rmat10")
+    base = _prepare(tmp_path, g, "rmat10")
+    a, b, R, L = 7, 9, 20, 11
+    r = _run_app("simrank", ["file", base, "a", str(a), "b", str(b), "R", str(R), "L", str(L),
+                             "blocksize_kb", str(int(g["blocksize_kb"])), "gw_walk_id", "source",
+                             "seed", str(int(g["seed"]))], tmp_path)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = float(re.search(r"SimRank for \d+ and \d+ = (\S+)", r.stdout).group(1))
+    gp = g["simrank_paths"]
+    fa, fb = gp[a], gp[b]
+    sim = np.float32(0.0)
+    for i in range(R):
+        for j in range(R):
+            for l in range(L):
+                if fa[i * L + l] == fb[j * L + l] and fa[i * L + l] != 0xFFFFFFFF:
+                    sim = np.float32(float(sim) + (1.0 / (R * R)) * 0.8 ** l)
+                    break
+    assert got == pytest.approx(float(sim), rel=1e-5, abs=1e-7)
+
+
+@pytest.mark.gpu
+def test_unchanged_rwdomination_graphlet_kkppr_apps(cuda_device, tmp_path):
+    g = load_golden("rmat10")
+    base = _prepare(tmp_path, g, "rmat10")
+    kb = str(int(g["blocksize_kb"]))
+    r = _run_app("rwdomination", ["file", base, "N", "1024", "R", "2", "L", "10", "blocksize_kb", kb], tmp_path)
+    assert r.returncode == 0, r.stderr[-2000:]
+    metrics = (tmp_path / "graphwalker_metrics.txt").read_text()
+    assert "00_runtime=" in metrics and "5_exec_updates=" in metrics
+    assert (tmp_path / "graphwalker_metrics.txt.statistics").read_text().strip()
+    r = _run_app("graphlet", ["file", base, "N", "1024", "R", "5000", "L", "4", "blocksize_kb", kb], tmp_path)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "cnt_all:\t5000" in r.stdout
+    ok = int(re.search(r"cnt_ok:\t(\d+)", r.stdout).group(1))
+    assert 0 <= ok <= 5000
+    r = _run_app("kk_ppr", ["file", base, "firstsource", "3", "numsources", "4", "walkspersource", "500",
+                            "blocksize_kb", kb], tmp_path)
+    assert r.returncode == 0, r.stderr[-2000:]
+    r = _run_app("rawrandomwalks", ["file", base, "N", "1024", "R", "3000", "L", "6", "blocksize_kb", kb], tmp_path)
+    assert r.returncode == 0, r.stderr[-2000:]
