@@ -33,7 +33,12 @@ class WalkParams(Structure):
                 ("jump_prob", c_double), ("seed", c_uint64), ("mode", c_uint32),
                 ("path_stride", c_uint32), ("max_hops", c_uint32), ("prob", c_float),
                 ("aggregate", c_uint32), ("max_supersteps", c_uint32), ("cache_hints", c_uint32),
-                ("reserved", c_uint32 * 5)]
+                ("table_factor", c_uint32), ("reserved", c_uint32 * 4)]
+
+
+class PprStats(Structure):
+    _fields_ = [("walks", c_uint64), ("table_slots", c_uint64), ("launches", c_uint32), ("reserved", c_uint32),
+                ("ms_clear", c_double), ("ms_walk", c_double), ("ms_topk", c_double), ("ms_total", c_double)]
 
 
 HINT_EXPLICIT = 0x80000000
@@ -94,6 +99,9 @@ _SIGS = {
     "gw_sync": (c_int32, [_P, _P]),
     "gw_probe_gather": (c_int32, [_P, _P, c_uint64, c_uint64, ctypes.c_int, POINTER(c_double)]),
     "gw_superstep_static": (c_int32, [_P, POINTER(WalkParams), c_uint32, _P, c_uint64, _P, _P, _P, _P, _P]),
+    "gw_ppr_run": (c_int32, [_P, POINTER(WalkParams), _P, _P, c_uint32, c_uint32, c_uint32, _P, _P,
+                             POINTER(PprStats)]),
+    "gw_ppr_autotune": (c_int32, [_P, POINTER(WalkParams), _P, _P, c_uint32, POINTER(c_uint32)]),
     "gw_set_l2_fetch_granularity": (c_int32, [_P, c_uint32, POINTER(c_uint32)]),
     "gw_set_l2_persisting": (c_int32, [_P, c_uint64]),
 }

@@ -397,7 +397,9 @@ gw_status gw_close(gw_ctx* ctx) {
                        &ctx->d_walks, &ctx->d_words, &ctx->d_ids, &ctx->d_counts, &ctx->d_paths,
                        &ctx->d_plen, &ctx->d_closure, &ctx->d_pool_offsets, &ctx->d_dest,
                        &ctx->d_tile_hist, &ctx->d_tile_off, &ctx->d_totals, &ctx->d_minhop,
-                       &ctx->d_scan_temp, &ctx->d_out_ptr, &ctx->d_out_base})
+                       &ctx->d_scan_temp, &ctx->d_out_ptr, &ctx->d_out_base, &ctx->d_q_sources,
+                       &ctx->d_q_prefix, &ctx->d_q_idbase, &ctx->d_q_toff, &ctx->d_q_tmask, &ctx->d_q_tables,
+                       &ctx->d_q_full, &ctx->d_q_ids, &ctx->d_q_counts})
     b->release();
   for (gw_devbuf& b : ctx->pools) b.release();
   ctx->h_rowptr.release();

@@ -98,6 +98,11 @@ struct gw_ctx {
   // L2 persisting reservation for the visit counters (0 = none)
   uint64_t l2_persist_bytes = 0;
 
+  // multi-source PPR queries
+  gw_devbuf d_q_sources, d_q_prefix, d_q_idbase, d_q_toff, d_q_tmask, d_q_tables, d_q_full, d_q_ids,
+      d_q_counts;
+  int ppr_threads_per_sm = 0;  // autotuned launch shape (0 = full occupancy)
+
   std::string err;
 
   // Access policy window over `counts` when an L2 reservation is active.

@@ -132,9 +132,22 @@ __device__ __forceinline__ L2Hints make_hints(uint32_t flags) {
 }
 
 template <int RULE>
+__device__ __forceinline__ bool hop_advance_rec(const GraphView& g, const WalkArgs& a, const L2Hints& hp,
+                                                uint32_t id, uint32_t src, uint32_t hop, uint32_t& v,
+                                                unsigned long long rec);
+
+template <int RULE>
 __device__ __forceinline__ bool hop_advance(const GraphView& g, const WalkArgs& a, const L2Hints& hp,
                                             uint32_t id, uint32_t src, uint32_t hop, uint32_t& v) {
-  const unsigned long long rec = ld_nc_u64(g.vrec + v, hp.rec);
+  return hop_advance_rec<RULE>(g, a, hp, id, src, hop, v, ld_nc_u64(g.vrec + v, hp.rec));
+}
+
+// The hop with v's packed record already loaded (callers that have other
+// memory work per visit issue the record load first to overlap the two).
+template <int RULE>
+__device__ __forceinline__ bool hop_advance_rec(const GraphView& g, const WalkArgs& a, const L2Hints& hp,
+                                                uint32_t id, uint32_t src, uint32_t hop, uint32_t& v,
+                                                unsigned long long rec) {
   const Philox4 ph = philox4x32_10(id, hop, 0u, 0u, a.seed_lo, a.seed_hi);
   const uint32_t d0 = ph.x >> 1;
   const uint32_t d1 = ph.y >> 1;

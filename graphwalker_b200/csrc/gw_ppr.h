@@ -1,0 +1,32 @@
+// gw_ppr.h -- multi-source PPR kernels (per-query sparse counts + top-k).
+#pragma once
+
+#include "gw_internal.h"
+
+namespace gw {
+
+constexpr int kPprThreads = 256;
+constexpr int kTopkThreads = 512;
+constexpr uint32_t kTopkBuffer = 1024;  // candidate keys per CTA
+constexpr uint32_t kTopkMaxK = kTopkBuffer - kTopkThreads;
+
+struct QueryView {
+  const uint32_t* sources;                 // nq source vertices
+  const unsigned long long* walk_prefix;   // nq + 1: walks of query q = [prefix[q], prefix[q+1])
+  const unsigned long long* id_base;       // nq: stream id of query q's first walk (NULL = prefix)
+  const unsigned long long* table_off;     // nq: first slot of query q's table
+  const uint32_t* table_mask;              // nq: table size - 1 (power of two)
+  unsigned long long* tables;              // all tables, slots (vertex << 32 | count), ~0 = empty
+  uint32_t* full;                          // nq: set to 1 when query q's table filled up
+  uint32_t nq;
+};
+
+// Walks [w_begin, w_end) of the batch; threads_per_sm <= 0 = full occupancy.
+cudaError_t launch_walk_queries(int rule, const QueryView& qv, unsigned long long w_begin,
+                                unsigned long long w_end, const GraphView& g, const WalkArgs& a,
+                                uint32_t* status, int threads_per_sm, cudaStream_t stream);
+// Top-k of queries [q_begin, q_begin + q_count) into out[q * k + r].
+cudaError_t launch_topk(const QueryView& qv, uint32_t q_begin, uint32_t q_count, uint32_t k, uint32_t* out_ids,
+                        uint32_t* out_counts, cudaStream_t stream);
+
+}  // namespace gw

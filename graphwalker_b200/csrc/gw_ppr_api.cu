@@ -1,0 +1,266 @@
+// gw_ppr_api.cu -- C ABI of the multi-source PPR queries (gw_ppr_run,
+// gw_ppr_autotune); the kernels are in gw_ppr.cu.
+//
+// Tables are sized for the typical query (table_factor slots per walk of the
+// budget).  A query whose table fills up is flagged by the kernel and run
+// again, alone with the other flagged queries, with tables four times larger:
+// its walks keep their stream ids, so the retried result is exactly the one a
+// large enough table would have given.
+#include <algorithm>
+#include <vector>
+
+#include "gw_ctx.h"
+#include "gw_ppr.h"
+
+namespace {
+
+constexpr int kMaxRetries = 3;
+
+uint64_t next_pow2(uint64_t x) {
+  uint64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+// A set of queries laid out for one launch.  Its device buffers are the
+// context's (kept across calls) for the first round, its own for retries.
+struct QuerySet {
+  std::vector<uint32_t> sources, qmap;  // qmap: index in the caller's query list
+  std::vector<unsigned long long> prefix, id_base, toff;
+  std::vector<uint32_t> tmask;
+  uint64_t walks = 0, slots = 0;
+  gw_devbuf own[9];
+  gw_devbuf *d_sources, *d_prefix, *d_id_base, *d_toff, *d_tmask, *d_tables, *d_full, *d_ids, *d_cnt;
+  gw::QueryView qv{};
+
+  QuerySet(gw_ctx* ctx, bool use_ctx_buffers) {
+    gw_devbuf* b[9] = {&ctx->d_q_sources, &ctx->d_q_prefix, &ctx->d_q_idbase, &ctx->d_q_toff, &ctx->d_q_tmask,
+                       &ctx->d_q_tables, &ctx->d_q_full, &ctx->d_q_ids, &ctx->d_q_counts};
+    gw_devbuf** d[9] = {&d_sources, &d_prefix, &d_id_base, &d_toff, &d_tmask, &d_tables, &d_full, &d_ids, &d_cnt};
+    for (int i = 0; i < 9; ++i) *d[i] = use_ctx_buffers ? b[i] : &own[i];
+  }
+  ~QuerySet() {
+    for (auto& b : own) b.release();
+  }
+};
+
+gw_status plan_set(gw_ctx* ctx, const uint32_t* sources, const uint32_t* budgets, const unsigned long long* ids,
+                   const std::vector<uint32_t>& which, uint64_t factor, QuerySet* s) {
+  const uint32_t n = (uint32_t)which.size();
+  s->qmap = which;
+  s->sources.resize(n);
+  s->prefix.assign(n + 1, 0);
+  s->id_base.resize(n);
+  s->toff.resize(n);
+  s->tmask.resize(n);
+  s->slots = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint32_t q = which[i];
+    if (sources[q] >= ctx->nv) return ctx->fail(GW_E_INVALID, "query %u: source %u >= nvertices", q, sources[q]);
+    s->sources[i] = sources[q];
+    s->prefix[i + 1] = s->prefix[i] + budgets[q];
+    s->id_base[i] = ids[q];
+    const uint64_t cap = next_pow2(std::max<uint64_t>(256, (uint64_t)budgets[q] * factor));
+    if (cap > (1ull << 31)) return ctx->fail(GW_E_OVERFLOW, "query %u: visit table would exceed 2^31 slots", q);
+    s->toff[i] = s->slots;
+    s->tmask[i] = (uint32_t)(cap - 1);
+    s->slots += cap;
+  }
+  s->walks = s->prefix[n];
+  return GW_OK;
+}
+
+gw_status upload_set(gw_ctx* ctx, QuerySet* s, uint32_t k, cudaStream_t st) {
+  const uint32_t n = (uint32_t)s->qmap.size();
+  GW_CUDA(ctx, s->d_sources->ensure(n * 4), "query alloc");
+  GW_CUDA(ctx, s->d_prefix->ensure((n + 1) * 8), "query alloc");
+  GW_CUDA(ctx, s->d_id_base->ensure(n * 8), "query alloc");
+  GW_CUDA(ctx, s->d_toff->ensure(n * 8), "query alloc");
+  GW_CUDA(ctx, s->d_tmask->ensure(n * 4), "query alloc");
+  GW_CUDA(ctx, s->d_tables->ensure(s->slots * 8), "query tables alloc");
+  GW_CUDA(ctx, s->d_full->ensure(n * 4), "query alloc");
+  GW_CUDA(ctx, s->d_ids->ensure((uint64_t)n * k * 4), "top-k alloc");
+  GW_CUDA(ctx, s->d_cnt->ensure((uint64_t)n * k * 4), "top-k alloc");
+  GW_CUDA(ctx, cudaMemcpyAsync(s->d_sources->p, s->sources.data(), n * 4, cudaMemcpyHostToDevice, st), "copy");
+  GW_CUDA(ctx, cudaMemcpyAsync(s->d_prefix->p, s->prefix.data(), (n + 1) * 8, cudaMemcpyHostToDevice, st), "copy");
+  GW_CUDA(ctx, cudaMemcpyAsync(s->d_id_base->p, s->id_base.data(), n * 8, cudaMemcpyHostToDevice, st), "copy");
+  GW_CUDA(ctx, cudaMemcpyAsync(s->d_toff->p, s->toff.data(), n * 8, cudaMemcpyHostToDevice, st), "copy");
+  GW_CUDA(ctx, cudaMemcpyAsync(s->d_tmask->p, s->tmask.data(), n * 4, cudaMemcpyHostToDevice, st), "copy");
+  GW_CUDA(ctx, cudaMemsetAsync(s->d_full->p, 0, n * 4, st), "clear flags");
+  s->qv.sources = s->d_sources->as<uint32_t>();
+  s->qv.walk_prefix = s->d_prefix->as<unsigned long long>();
+  s->qv.id_base = s->d_id_base->as<unsigned long long>();
+  s->qv.table_off = s->d_toff->as<unsigned long long>();
+  s->qv.table_mask = s->d_tmask->as<uint32_t>();
+  s->qv.tables = s->d_tables->as<unsigned long long>();
+  s->qv.full = s->d_full->as<uint32_t>();
+  s->qv.nq = n;
+  return GW_OK;
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  return ms;
+}
+
+// Clear + walk + top-k of a whole set in three launches (batched) or query by
+// query (plain).  Timing events: ev[0] start, ev[1] cleared, ev[2] walked, ev[3] done.
+cudaError_t run_set(gw_ctx* ctx, const gw_walk_params* p, const gw::WalkArgs& a, QuerySet* s, uint32_t k,
+                    bool batched, int threads_per_sm, cudaStream_t st, cudaEvent_t* ev, uint32_t* launches) {
+  cudaError_t e = cudaSuccess;
+  const uint32_t n = s->qv.nq;
+  cudaEventRecord(ev[0], st);
+  if (batched) {
+    e = cudaMemsetAsync(s->qv.tables, 0xff, s->slots * 8, st);
+    cudaEventRecord(ev[1], st);
+    if (e == cudaSuccess)
+      e = gw::launch_walk_queries((int)p->rule, s->qv, 0, s->walks, ctx->view(), a, ctx->d_status.as<uint32_t>(),
+                                  threads_per_sm, st);
+    cudaEventRecord(ev[2], st);
+    if (e == cudaSuccess) e = gw::launch_topk(s->qv, 0, n, k, s->d_ids->as<uint32_t>(), s->d_cnt->as<uint32_t>(), st);
+    cudaEventRecord(ev[3], st);
+    *launches += 3;
+  } else {
+    cudaEventRecord(ev[1], st);
+    for (uint32_t q = 0; q < n && e == cudaSuccess; ++q) {
+      e = cudaMemsetAsync(s->qv.tables + s->toff[q], 0xff, ((uint64_t)s->tmask[q] + 1) * 8, st);
+      if (e == cudaSuccess)
+        e = gw::launch_walk_queries((int)p->rule, s->qv, s->prefix[q], s->prefix[q + 1], ctx->view(), a,
+                                    ctx->d_status.as<uint32_t>(), 0, st);
+      if (e == cudaSuccess) e = gw::launch_topk(s->qv, q, 1, k, s->d_ids->as<uint32_t>(), s->d_cnt->as<uint32_t>(), st);
+    }
+    cudaEventRecord(ev[2], st);
+    cudaEventRecord(ev[3], st);
+    *launches += 3 * n;
+  }
+  return e;
+}
+
+}  // namespace
+
+extern "C" gw_status gw_ppr_run(gw_ctx* ctx, const gw_walk_params* params, const uint32_t* sources,
+                                const uint32_t* budgets, uint32_t nq, uint32_t k, uint32_t batched,
+                                uint32_t* topk_ids, uint32_t* topk_counts, gw_ppr_stats* stats) {
+  if (!ctx) return GW_E_INVALID;
+  if (ctx->residency != GW_RESIDENT_HBM) return ctx->fail(GW_E_STATE, "PPR queries need a resident graph");
+  if (nq == 0) return GW_OK;
+  if (!sources || !budgets || !topk_ids || !topk_counts) return ctx->fail(GW_E_INVALID, "NULL buffer");
+  if (k == 0 || k > gw::kTopkMaxK) return ctx->fail(GW_E_INVALID, "k must lie in [1, %u]", gw::kTopkMaxK);
+  gw::WalkArgs a;
+  gw_status s = gw::make_walk_args(ctx, params, &a);
+  if (s != GW_OK) return s;
+  // stream id of each query's first walk: budgets laid end to end
+  std::vector<unsigned long long> ids(nq);
+  unsigned long long total = 0;
+  for (uint32_t q = 0; q < nq; ++q) {
+    ids[q] = total;
+    total += budgets[q];
+  }
+  std::vector<uint32_t> which(nq);
+  for (uint32_t q = 0; q < nq; ++q) which[q] = q;
+  uint64_t factor = params->table_factor ? params->table_factor : 8;
+  cudaStream_t st = ctx->stream;
+  cudaEvent_t ev[4];
+  for (auto& e : ev) cudaEventCreate(&e);
+  gw_ppr_stats local{};
+  local.walks = total;
+  std::vector<uint32_t> full, hid, hcnt;
+  for (int round = 0; round <= kMaxRetries && !which.empty(); ++round) {
+    QuerySet set(ctx, round == 0);
+    s = plan_set(ctx, sources, budgets, ids.data(), which, factor, &set);
+    if (s == GW_OK) s = upload_set(ctx, &set, k, st);
+    if (s != GW_OK) break;
+    const bool b = batched || round > 0;
+    cudaError_t e = run_set(ctx, params, a, &set, k, b, b ? ctx->ppr_threads_per_sm : 0, st, ev, &local.launches);
+    const uint32_t n = (uint32_t)which.size();
+    full.resize(n);
+    hid.resize((size_t)n * k);
+    hcnt.resize((size_t)n * k);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(full.data(), set.d_full->p, n * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hid.data(), set.d_ids->p, (size_t)n * k * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hcnt.data(), set.d_cnt->p, (size_t)n * k * 4, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) {
+      s = ctx->cuda_fail(e, "gw_ppr_run");
+      break;
+    }
+    s = gw::take_status(ctx, st);
+    if (s != GW_OK) break;
+    if (round == 0 && b) {
+      local.ms_clear = elapsed(ev[0], ev[1]);
+      local.ms_walk = elapsed(ev[1], ev[2]);
+      local.ms_topk = elapsed(ev[2], ev[3]);
+    }
+    local.ms_total += elapsed(ev[0], ev[3]);
+    local.table_slots += set.slots;
+    std::vector<uint32_t> again;
+    for (uint32_t i = 0; i < n; ++i) {
+      const uint32_t q = which[i];
+      if (full[i]) {
+        again.push_back(q);
+        continue;
+      }
+      std::copy(hid.begin() + (size_t)i * k, hid.begin() + (size_t)(i + 1) * k, topk_ids + (size_t)q * k);
+      std::copy(hcnt.begin() + (size_t)i * k, hcnt.begin() + (size_t)(i + 1) * k, topk_counts + (size_t)q * k);
+    }
+    which.swap(again);
+    factor *= 4;
+  }
+  for (auto& x : ev) cudaEventDestroy(x);
+  if (s == GW_OK && !which.empty())
+    s = ctx->fail(GW_E_OVERFLOW, "%zu queries still filled their visit tables after %d retries",
+                  which.size(), kMaxRetries);
+  if (stats) *stats = local;
+  return s;
+}
+
+extern "C" gw_status gw_ppr_autotune(gw_ctx* ctx, const gw_walk_params* params, const uint32_t* sources,
+                                     const uint32_t* budgets, uint32_t nq, uint32_t* threads_per_sm) {
+  if (!ctx) return GW_E_INVALID;
+  if (nq == 0 || !sources || !budgets) return ctx->fail(GW_E_INVALID, "empty sample");
+  gw::WalkArgs a;
+  gw_status s = gw::make_walk_args(ctx, params, &a);
+  if (s != GW_OK) return s;
+  std::vector<unsigned long long> ids(nq);
+  unsigned long long total = 0;
+  for (uint32_t q = 0; q < nq; ++q) {
+    ids[q] = total;
+    total += budgets[q];
+  }
+  std::vector<uint32_t> which(nq);
+  for (uint32_t q = 0; q < nq; ++q) which[q] = q;
+  QuerySet set(ctx, true);
+  s = plan_set(ctx, sources, budgets, ids.data(), which, params->table_factor ? params->table_factor : 8, &set);
+  if (s == GW_OK) s = upload_set(ctx, &set, 1, ctx->stream);
+  if (s != GW_OK) return s;
+  cudaStream_t st = ctx->stream;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int candidates[] = {512, 1024, 1536, 2048};
+  int best = 0;
+  float best_ms = 1e30f;
+  for (int c : candidates) {
+    float ms_sum = 0.f;
+    for (int rep = 0; rep < 3; ++rep) {
+      cudaMemsetAsync(set.qv.tables, 0xff, set.slots * 8, st);
+      cudaEventRecord(e0, st);
+      gw::launch_walk_queries((int)params->rule, set.qv, 0, set.walks, ctx->view(), a, ctx->d_status.as<uint32_t>(),
+                              c, st);
+      cudaEventRecord(e1, st);
+      cudaEventSynchronize(e1);
+      if (rep) ms_sum += elapsed(e0, e1);  // the first run warms up
+    }
+    if (ms_sum < best_ms) {
+      best_ms = ms_sum;
+      best = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  s = gw::take_status(ctx, st);
+  if (s != GW_OK) return s;
+  ctx->ppr_threads_per_sm = best;
+  if (threads_per_sm) *threads_per_sm = (uint32_t)best;
+  return GW_OK;
+}

@@ -229,6 +229,27 @@ class Graph:
     def sync(self, stream: int | None = None) -> None:
         check(load().gw_sync(self._h, stream), self._h)
 
+    # ---- multi-source PPR queries ----
+    def ppr(self, p: WalkParams, sources, budgets, k: int = 100, batched: bool = True):
+        """Top-k (ids, counts) per query, shape (nq, k), and the run's PprStats."""
+        sources = np.ascontiguousarray(sources, dtype=np.uint32)
+        budgets = np.ascontiguousarray(budgets, dtype=np.uint32)
+        nq = len(sources)
+        ids = np.zeros(nq * k, dtype=np.uint32)
+        counts = np.zeros(nq * k, dtype=np.uint32)
+        st = _lib.PprStats()
+        check(load().gw_ppr_run(self._h, byref(p), _ptr(sources), _ptr(budgets), nq, k, int(batched), _ptr(ids),
+                                _ptr(counts), byref(st)), self._h)
+        return ids.reshape(nq, k), counts.reshape(nq, k), st
+
+    def ppr_autotune(self, p: WalkParams, sources, budgets) -> int:
+        sources = np.ascontiguousarray(sources, dtype=np.uint32)
+        budgets = np.ascontiguousarray(budgets, dtype=np.uint32)
+        out = c_uint32()
+        check(load().gw_ppr_autotune(self._h, byref(p), _ptr(sources), _ptr(budgets), len(sources), byref(out)),
+              self._h)
+        return out.value
+
     def set_l2_fetch_granularity(self, nbytes: int) -> int:
         """Sets the context's L2 fetch granularity (0 = leave); returns the old one."""
         old = c_uint32()

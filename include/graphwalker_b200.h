@@ -98,7 +98,9 @@ typedef struct gw_walk_params {
                               until no walk is pending)                        */
   uint32_t cache_hints; /* L2 eviction priorities of the walk kernels: 0 = the
                            engine default; otherwise GW_HINT_EXPLICIT | bits  */
-  uint32_t reserved[5];
+  uint32_t table_factor; /* PPR queries: table slots per walk of the budget,
+                            rounded up to a power of two (0 = 8)           */
+  uint32_t reserved[4];
 } gw_walk_params;
 
 typedef struct gw_run_stats {
@@ -189,6 +191,37 @@ gw_status gw_read_pool(gw_ctx *ctx, uint32_t block, gw_walk_rec *out, size_t cap
    (VERTEX_COUNT sink; counts is overwritten).  ids may be NULL.            */
 gw_status gw_run_pools(gw_ctx *ctx, const gw_walk_params *params, const uint64_t *words,
                        const uint64_t *pool_offsets, const uint32_t *ids, uint32_t *counts);
+
+/* ---- multi-source PPR queries (msppr, apps/msppr.cpp:25-145) ------------ */
+typedef struct gw_ppr_stats {
+  uint64_t walks;        /* walks run                                          */
+  uint64_t table_slots;  /* per-query table slots allocated                    */
+  uint32_t launches;     /* kernels + clears issued                            */
+  uint32_t reserved;
+  double ms_clear;       /* device time clearing tables                        */
+  double ms_walk;        /* device time of the walk kernels                    */
+  double ms_topk;        /* device time of the top-k kernels                   */
+  double ms_total;       /* device time of the whole call (first to last op)   */
+} gw_ppr_stats;
+
+/* Runs budgets[q] walks from sources[q] for each of nq queries with the
+   walk class of params->rule (msppr: GW_RULE_STOP, L = maxwalklength) and
+   returns each query's top k visited vertices: topk_ids[q*k + r] by visit
+   count, ties broken by the smaller vertex id (0xffffffff / 0 pad a short
+   list); k <= 512.  Walk j of the batch (queries in order, budgets laid end
+   to end) uses stream id j, so a query's result does not depend on the
+   other queries.  batched = 1: all queries in one persistent walk launch and
+   one top-k launch (the replacement of msppr's per-source
+   DiscreteDistribution); batched = 0: one query at a time (clear, walk,
+   top-k per query) -- the plain per-query path.  stats may be NULL.      */
+gw_status gw_ppr_run(gw_ctx *ctx, const gw_walk_params *params, const uint32_t *sources,
+                     const uint32_t *budgets, uint32_t nq, uint32_t k, uint32_t batched,
+                     uint32_t *topk_ids, uint32_t *topk_counts, gw_ppr_stats *stats);
+/* Times candidate launch shapes of the batched query kernel on the given
+   queries (a sample of the workload) and keeps the fastest for this
+   context; *threads_per_sm receives the choice.                            */
+gw_status gw_ppr_autotune(gw_ctx *ctx, const gw_walk_params *params, const uint32_t *sources,
+                          const uint32_t *budgets, uint32_t nq, uint32_t *threads_per_sm);
 
 /* ---- device-pointer entry points (stream-ordered) ----------------------- */
 /* Runs n walks resident in HBM over the whole resident graph.  Sink buffers
