@@ -61,8 +61,11 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-probe", action="store_true", help="skip the random-gather roof probe")
     ap.add_argument("--cpu-sample-sec", type=float, default=15.0)
-    ap.add_argument("--workload", choices=["rawwalk", "msppr"], default="rawwalk",
-                    help="rawwalk: the headline raw-random-walk step; msppr: batched vs plain multi-source PPR")
+    ap.add_argument("--workload", choices=["rawwalk", "msppr", "serve"], default="rawwalk",
+                    help="rawwalk: the headline raw-random-walk step; msppr: batched vs plain multi-source PPR; "
+                         "serve: Poisson-arrival PPR serving, continuous batching vs one query per launch")
+    ap.add_argument("--rates", default="1000,5000,10000,20000,50000", help="serve: arrival rates (queries/s)")
+    ap.add_argument("--serve-sec", type=float, default=2.0, help="serve: seconds of arrivals per rate")
     ap.add_argument("--queries", type=int, default=4096)
     ap.add_argument("--topk", type=int, default=100)
     return ap.parse_args()
@@ -472,12 +475,65 @@ def msppr_arm(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def serve_arm(args) -> None:
+    """PPR serving on one GPU: Poisson arrivals at each rate, budgets
+    Pareto(alpha=1.5, x_m=100) clipped to [100, 1e6], top-100 per query;
+    continuous batching vs the plain one-query-per-superstep server."""
+    import numpy as np
+    import torch
+
+    import graphwalker_b200 as gw
+    torch.cuda.set_device(0)
+    scale = args.scale if args.scale != 24 else 26
+    G = gw.Graph.rmat(scale, args.edge_factor, seed=args.graph_seed,
+                      blocksize_kb=blocksize_kb_for(scale, args.edge_factor, args.nblocks))
+    rp, _ = G.export_csr()
+    deg = np.diff(rp.astype(np.int64))
+    cand = np.nonzero(deg > 0)[0]
+    del rp, deg
+    p = gw.params(gw.RULE_STOP, gw.SINK_NONE, 20, seed=args.walk_seed)
+    rng = np.random.default_rng(11)
+    G.ppr_autotune(p, rng.choice(cand, 64).astype(np.uint32), np.full(64, 2000, np.uint32))
+    results = []
+    for rate in [float(r) for r in args.rates.split(",")]:
+        n = max(200, int(rate * args.serve_sec))
+        src = rng.choice(cand, n).astype(np.uint32)
+        bud = np.clip(np.round(100.0 / rng.random(n) ** (1 / 1.5)), 100, 1_000_000).astype(np.uint32)
+        gaps = rng.exponential(1e9 / rate, n)
+        row = {"rate_qps": rate, "queries": n, "mean_budget": float(bud.mean())}
+        for name, mode in (("batched", gw._lib.SERVE_BATCHED), ("plain", gw._lib.SERVE_PLAIN)):
+            with G.serve(p, k=args.topk, mode=mode, table_slots=1 << 30) as S:
+                S.wait(S.submit(int(src[0]), 1000, 0))  # warm-up
+                t0 = S.clock_ns() + 5_000_000
+                arrivals = t0 + np.cumsum(gaps).astype(np.int64)
+                tickets = [S.submit(int(s), int(b), i, int(a)) for i, (s, b, a) in enumerate(zip(src, bud, arrivals))]
+                tm = [S.wait(t)[2] for t in tickets]
+                st = S.stats()
+            lat = np.array([x.done_ns - x.arrival_ns for x in tm], dtype=np.float64) / 1e6
+            span = (max(x.done_ns for x in tm) - int(arrivals[0])) / 1e9
+            row[name] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                         "throughput_qps": n / span, "supersteps": int(st.supersteps)}
+        results.append(row)
+        print(json.dumps(row), flush=True)
+    best = max(results, key=lambda r: r["batched"]["throughput_qps"])
+    line = {"metric": "queries/s", "value": best["batched"]["throughput_qps"], "unit": "queries/s",
+            "workload": "serve", "n_gpus": 1, "steps": len(results), "warmup": 1, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": f"PPR serving, R-MAT scale {scale}, Poisson arrivals, budgets Pareto(1.5, 100) "
+                                   f"clipped to [100, 1e6], stop rule p=0.15, L<=20, top-{args.topk}"},
+            "rates": results}
+    G.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         reference_arm(args)
     elif args.workload == "msppr":
         msppr_arm(args)
+    elif args.workload == "serve":
+        serve_arm(args)
     else:
         our_arm(args)
 

@@ -36,6 +36,24 @@ class WalkParams(Structure):
                 ("table_factor", c_uint32), ("reserved", c_uint32 * 4)]
 
 
+SERVE_BATCHED, SERVE_PLAIN = 0, 1
+
+
+class ServeConfig(Structure):
+    _fields_ = [("table_slots", c_uint64), ("max_walks_per_step", c_uint32), ("quantum", c_uint32),
+                ("k", c_uint32), ("mode", c_uint32), ("reserved", c_uint32 * 4)]
+
+
+class ServeTiming(Structure):
+    _fields_ = [("arrival_ns", c_uint64), ("admit_ns", c_uint64), ("done_ns", c_uint64), ("restarts", c_uint32),
+                ("reserved", c_uint32)]
+
+
+class ServeStats(Structure):
+    _fields_ = [("submitted", c_uint64), ("completed", c_uint64), ("supersteps", c_uint64), ("walks", c_uint64),
+                ("restarts", c_uint64), ("pending", c_uint64), ("active", c_uint64)]
+
+
 class PprStats(Structure):
     _fields_ = [("walks", c_uint64), ("table_slots", c_uint64), ("launches", c_uint32), ("reserved", c_uint32),
                 ("ms_clear", c_double), ("ms_walk", c_double), ("ms_topk", c_double), ("ms_total", c_double)]
@@ -102,6 +120,12 @@ _SIGS = {
     "gw_ppr_run": (c_int32, [_P, POINTER(WalkParams), _P, _P, c_uint32, c_uint32, c_uint32, _P, _P,
                              POINTER(PprStats)]),
     "gw_ppr_autotune": (c_int32, [_P, POINTER(WalkParams), _P, _P, c_uint32, POINTER(c_uint32)]),
+    "gw_serve_open": (c_int32, [_P, POINTER(WalkParams), POINTER(ServeConfig), POINTER(c_void_p)]),
+    "gw_serve_submit": (c_int32, [_P, c_uint32, c_uint32, c_uint32, c_uint64, POINTER(c_uint64)]),
+    "gw_serve_wait": (c_int32, [_P, c_uint64, ctypes.c_int64, _P, _P, POINTER(ServeTiming)]),
+    "gw_serve_get_stats": (c_int32, [_P, POINTER(ServeStats)]),
+    "gw_serve_clock_ns": (c_uint64, []),
+    "gw_serve_close": (c_int32, [_P]),
     "gw_set_l2_fetch_granularity": (c_int32, [_P, c_uint32, POINTER(c_uint32)]),
     "gw_set_l2_persisting": (c_int32, [_P, c_uint64]),
 }

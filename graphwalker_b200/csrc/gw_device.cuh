@@ -134,7 +134,7 @@ __device__ __forceinline__ L2Hints make_hints(uint32_t flags) {
 template <int RULE>
 __device__ __forceinline__ bool hop_advance_rec(const GraphView& g, const WalkArgs& a, const L2Hints& hp,
                                                 uint32_t id, uint32_t src, uint32_t hop, uint32_t& v,
-                                                unsigned long long rec);
+                                                unsigned long long rec, uint32_t stream = 0u);
 
 template <int RULE>
 __device__ __forceinline__ bool hop_advance(const GraphView& g, const WalkArgs& a, const L2Hints& hp,
@@ -144,11 +144,13 @@ __device__ __forceinline__ bool hop_advance(const GraphView& g, const WalkArgs& 
 
 // The hop with v's packed record already loaded (callers that have other
 // memory work per visit issue the record load first to overlap the two).
+// `stream` is the third Philox counter word: 0 for walks keyed by a global
+// walk id; a served query's own stream id otherwise.
 template <int RULE>
 __device__ __forceinline__ bool hop_advance_rec(const GraphView& g, const WalkArgs& a, const L2Hints& hp,
                                                 uint32_t id, uint32_t src, uint32_t hop, uint32_t& v,
-                                                unsigned long long rec) {
-  const Philox4 ph = philox4x32_10(id, hop, 0u, 0u, a.seed_lo, a.seed_hi);
+                                                unsigned long long rec, uint32_t stream) {
+  const Philox4 ph = philox4x32_10(id, hop, stream, 0u, a.seed_lo, a.seed_hi);
   const uint32_t d0 = ph.x >> 1;
   const uint32_t d1 = ph.y >> 1;
   unsigned long long off = rec >> kDegBits;

@@ -78,6 +78,7 @@ __global__ void __launch_bounds__(kPprThreads)
   uint32_t src = __ldg(qv.sources + q);
   // stream id = the walk's position in the original batch
   unsigned long long id_shift = qv.id_base ? __ldg(qv.id_base + q) - __ldg(qv.walk_prefix + q) : 0ull;
+  uint32_t sid = qv.stream ? __ldg(qv.stream + q) : 0u;
   uint32_t v = src, hop = 0, st = 0;
   for (;;) {
     bool end;
@@ -100,7 +101,7 @@ __global__ void __launch_bounds__(kPprThreads)
         unsigned long long* t = qv.tables + __ldg(qv.table_off + q);
         if (!table_add(t, __ldg(qv.table_mask + q), v, (uint32_t)__popc(peers))) qv.full[q] = 1u;
       }
-      end = !hop_advance_rec<RULE>(g, a, hp, (uint32_t)(j + id_shift), src, hop, v, rec);
+      end = !hop_advance_rec<RULE>(g, a, hp, (uint32_t)(j + id_shift), src, hop, v, rec, sid);
       if (!end) {
         ++hop;
         if (RULE == GW_RULE_RESTART && hop % a.L == a.L - 1) end = true;
@@ -113,6 +114,7 @@ __global__ void __launch_bounds__(kPprThreads)
         q = query_of(qv.walk_prefix, qv.nq, j);
         src = __ldg(qv.sources + q);
         id_shift = qv.id_base ? __ldg(qv.id_base + q) - __ldg(qv.walk_prefix + q) : 0ull;
+        sid = qv.stream ? __ldg(qv.stream + q) : 0u;
       }
       v = src;
       hop = 0;

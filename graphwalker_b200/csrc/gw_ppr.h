@@ -18,6 +18,7 @@ struct QueryView {
   const uint32_t* table_mask;              // nq: table size - 1 (power of two)
   unsigned long long* tables;              // all tables, slots (vertex << 32 | count), ~0 = empty
   uint32_t* full;                          // nq: set to 1 when query q's table filled up
+  const uint32_t* stream;                  // nq: Philox stream word of query q (NULL = 0)
   uint32_t nq;
 };
 

@@ -250,6 +250,10 @@ class Graph:
               self._h)
         return out.value
 
+    def serve(self, p: WalkParams, k: int = 100, mode: int = _lib.SERVE_BATCHED, table_slots: int = 0,
+              max_walks_per_step: int = 0, quantum: int = 0) -> "Server":
+        return Server(self, p, k, mode, table_slots, max_walks_per_step, quantum)
+
     def set_l2_fetch_granularity(self, nbytes: int) -> int:
         """Sets the context's L2 fetch granularity (0 = leave); returns the old one."""
         old = c_uint32()
@@ -263,3 +267,49 @@ class Graph:
         out = c_double()
         check(load().gw_probe_gather(self._h, _ptr(buf), n_words, loads, iters, byref(out)), self._h)
         return out.value
+
+
+class Server:
+    """A continuous-batching PPR query server on one graph (gw_serve_*)."""
+
+    def __init__(self, graph: Graph, p: WalkParams, k: int, mode: int, table_slots: int, max_walks_per_step: int,
+                 quantum: int):
+        self.graph, self.k = graph, k
+        cfg = _lib.ServeConfig(table_slots, max_walks_per_step, quantum, k, mode)
+        h = c_void_p()
+        check(load().gw_serve_open(graph.handle, byref(p), byref(cfg), byref(h)), graph.handle)
+        self._h = h
+
+    @staticmethod
+    def clock_ns() -> int:
+        return load().gw_serve_clock_ns()
+
+    def submit(self, source: int, budget: int, stream: int = 0, arrival_ns: int = 0) -> int:
+        t = c_uint64()
+        check(load().gw_serve_submit(self._h, source, budget, stream, arrival_ns, byref(t)), self.graph.handle)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        """(ids[k], counts[k], ServeTiming) of a ticket."""
+        ids = np.zeros(self.k, dtype=np.uint32)
+        counts = np.zeros(self.k, dtype=np.uint32)
+        tm = _lib.ServeTiming()
+        check(load().gw_serve_wait(self._h, ticket, timeout_ms, _ptr(ids), _ptr(counts), byref(tm)),
+              self.graph.handle)
+        return ids, counts, tm
+
+    def stats(self) -> _lib.ServeStats:
+        s = _lib.ServeStats()
+        check(load().gw_serve_get_stats(self._h, byref(s)), self.graph.handle)
+        return s
+
+    def close(self) -> None:
+        if self._h:
+            load().gw_serve_close(self._h)
+            self._h = c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -223,6 +223,49 @@ gw_status gw_ppr_run(gw_ctx *ctx, const gw_walk_params *params, const uint32_t *
 gw_status gw_ppr_autotune(gw_ctx *ctx, const gw_walk_params *params, const uint32_t *sources,
                           const uint32_t *budgets, uint32_t nq, uint32_t *threads_per_sm);
 
+/* ---- serving PPR queries (continuous batching) --------------------------
+   No counterpart in the reference, which runs one batch of sources per
+   process.  A server owns its context's stream while open (make no other
+   calls on that context meanwhile).  Its scheduler thread admits arrived
+   queries while their visit tables fit in a device arena, and runs
+   supersteps that mix walk chunks of every admitted query; queries that
+   arrive while a superstep runs join the next one.  Query walk w uses Philox
+   counter (w, hop, stream, 0): a query's top-k depends only on (source,
+   budget, stream), alone or in any mix.                                     */
+typedef struct gw_server gw_server;
+#define GW_SERVE_BATCHED 0 /* continuous batching across queries            */
+#define GW_SERVE_PLAIN 1   /* one whole query per superstep (per-query path) */
+typedef struct gw_serve_config {
+  uint64_t table_slots;        /* table arena size in 8-byte slots (0 = 2^28)  */
+  uint32_t max_walks_per_step; /* walks per superstep (0 = 2^22)               */
+  uint32_t quantum;            /* walks of one query per superstep (0 = 2^16)  */
+  uint32_t k;                  /* top-k length (0 = 100, at most 512)          */
+  uint32_t mode;               /* GW_SERVE_BATCHED or GW_SERVE_PLAIN           */
+  uint32_t reserved[4];
+} gw_serve_config;
+typedef struct gw_serve_timing {
+  uint64_t arrival_ns, admit_ns, done_ns; /* gw_serve_clock_ns() time base    */
+  uint32_t restarts;                      /* table-full restarts               */
+  uint32_t reserved;
+} gw_serve_timing;
+typedef struct gw_serve_stats {
+  uint64_t submitted, completed, supersteps, walks, restarts, pending, active;
+} gw_serve_stats;
+gw_status gw_serve_open(gw_ctx *ctx, const gw_walk_params *params, const gw_serve_config *cfg,
+                        gw_server **out);
+/* Queues one query; arrival_ns = 0 means now, a later gw_serve_clock_ns()
+   time schedules it (open-loop load replay).                               */
+gw_status gw_serve_submit(gw_server *srv, uint32_t source, uint32_t budget, uint32_t stream,
+                          uint64_t arrival_ns, uint64_t *ticket);
+/* Waits (timeout_ms < 0: forever) and returns the top-k lists (k entries
+   each) and timing of a ticket, then forgets it; GW_E_TIMEOUT if not done. */
+gw_status gw_serve_wait(gw_server *srv, uint64_t ticket, int64_t timeout_ms, uint32_t *ids,
+                        uint32_t *counts, gw_serve_timing *timing);
+gw_status gw_serve_get_stats(gw_server *srv, gw_serve_stats *stats);
+uint64_t gw_serve_clock_ns(void);
+/* Finishes admitted queries, cancels queued ones (GW_E_STATE), frees all.   */
+gw_status gw_serve_close(gw_server *srv);
+
 /* ---- device-pointer entry points (stream-ordered) ----------------------- */
 /* Runs n walks resident in HBM over the whole resident graph.  Sink buffers
    by params->sink: d_counts[nvertices] (accumulated, not cleared),
