@@ -61,11 +61,12 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-probe", action="store_true", help="skip the random-gather roof probe")
     ap.add_argument("--cpu-sample-sec", type=float, default=15.0)
-    ap.add_argument("--workload", choices=["rawwalk", "msppr", "serve"], default="rawwalk",
+    ap.add_argument("--workload", choices=["rawwalk", "msppr", "serve", "ppr1", "ooc"], default="rawwalk",
                     help="rawwalk: the headline raw-random-walk step; msppr: batched vs plain multi-source PPR; "
                          "serve: Poisson-arrival PPR serving, continuous batching vs one query per launch")
     ap.add_argument("--rates", default="1000,5000,10000,20000,50000", help="serve: arrival rates (queries/s)")
     ap.add_argument("--serve-sec", type=float, default=2.0, help="serve: seconds of arrivals per rate")
+    ap.add_argument("--nmblocks", type=int, default=32, help="ooc: device block slots")
     ap.add_argument("--queries", type=int, default=4096)
     ap.add_argument("--topk", type=int, default=100)
     return ap.parse_args()
@@ -245,6 +246,34 @@ def cpu_reference(args, rowptr, colidx, warmup: int, steps: int, budget_s: float
                       f"native rand_r, {threads} OpenMP threads, one walk on every {stride}-th vertex "
                       f"({nv // stride} walks x {args.L} hops per run) of the same scale-{args.scale} graph, "
                       f"blocks cached in RAM after the first run"}
+
+
+def cpu_reference_msppr(args, rowptr, colidx, walkspersource: int, budget_s: float) -> dict:
+    """The reference engine with RandomWalkwithStop on msppr's placement
+    (contiguous sources, a fixed number of walks each), sized to budget_s."""
+    threads = host_cores()
+    exe = ROOT / "oracle" / "_ref" / "gw_ref_bench"
+    with tempfile.TemporaryDirectory(prefix="gw_ref_") as td:
+        tmp = Path(td)
+        base, kb, nb = write_reference_graph(tmp, args, rowptr, colidx)
+        nv = len(rowptr) - 1
+
+        def run(numsources: int, warm: int):
+            out = subprocess.run([str(exe), base, str(kb), str(nv), "20", "1", str(warm), "1", "execthreads",
+                                  str(threads), "msppr", "0", str(numsources), str(walkspersource)],
+                                 cwd=tmp, capture_output=True, text=True, timeout=1800)
+            if out.returncode != 0:
+                raise RuntimeError(out.stderr[-400:])
+            f = [l.split() for l in out.stdout.splitlines() if l.startswith("step")][-1]
+            return float(f[7]), int(f[5])
+
+        t_cal, _ = run(8, 1)
+        numsources = max(8, min(4096, int(8 * budget_s / max(t_cal, 1e-6))))
+        t, visits = run(numsources, 1)
+    return {"value": numsources / t, "unit": "queries/s", "cores": threads, "kind": "reference",
+            "sample": f"the reference engine + RandomWalkwithStop compiled -O3 from source, native rand_r, "
+                      f"{threads} OpenMP threads, msppr placement: sources 0..{numsources - 1} x {walkspersource} "
+                      f"walks (the mean budget), L<=20, a per-thread visit counter as sink ({visits} visits)"}
 
 
 def reference_arm(args) -> None:
@@ -454,6 +483,22 @@ def msppr_arm(args) -> None:
     t0 = time.perf_counter()
     G.ppr(p, sources, budgets, k=args.topk, batched=True)
     e2e_s = time.perf_counter() - t0
+    # top-100 accuracy against the FP64 power series, on the largest-budget queries
+    acc = []
+    for q in np.argsort(-budgets.astype(np.int64))[:4]:
+        mu = G.expected_visits(p, int(sources[q]))
+        exact = set(np.argsort(-mu, kind="stable")[:args.topk].tolist())
+        got = set(int(x) for x in ids_b[q] if x != 0xFFFFFFFF)
+        acc.append({"budget": int(budgets[q]), "top_overlap": len(exact & got)})
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            rp_h, ci_h = G.export_csr()
+            cpu = cpu_reference_msppr(args, rp_h, ci_h, int(round(float(budgets.mean()))), args.cpu_sample_sec)
+            del rp_h, ci_h
+        except Exception as exc:  # reported, never required
+            cpu = {"value": None, "unit": "queries/s", "cores": host_cores(), "kind": "reference",
+                   "sample": f"unavailable: {exc}"}
     line = {"metric": "queries/s", "value": args.queries / (ms_med * 1e-3), "unit": "queries/s",
             "workload": "msppr", "n_gpus": 1, "steps": args.steps, "warmup": max(1, args.warmup),
             "ms_per_step": ms_med, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -468,6 +513,7 @@ def msppr_arm(args) -> None:
             "plain": {"value": args.queries / (stp.ms_total * 1e-3), "unit": "queries/s", "ms": stp.ms_total,
                       "launches": stp.launches},
             "speedup_vs_plain": stp.ms_total / ms_med, "identical_to_plain": same,
+            "accuracy_vs_fp64": acc, "cpu_baseline": cpu,
             "e2e": {"value": args.queries / e2e_s, "unit": "queries/s", "api": "gw_ppr_run (host arrays)",
                     "h2d_bytes_per_step": int(args.queries * 8), "d2h_bytes_per_step": int(args.queries * args.topk * 8)},
             "gpu_launches": 3, "clocks": clk.summary()}
@@ -526,8 +572,127 @@ def serve_arm(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def ppr1_arm(args) -> None:
+    """Single-source PPR (R-MAT scale 20, 16 blocks, 100,000 walks from vertex
+    0, stop w.p. 0.15, a dangling vertex sends the walk back to its source,
+    at most 20 hops): per-vertex visit counts and the top-100, with the L1
+    error and top-100 overlap against the FP64 power series."""
+    import numpy as np
+    import torch
+
+    import graphwalker_b200 as gw
+    torch.cuda.set_device(0)
+    scale = 20 if args.scale == 24 else args.scale
+    B, L = 100_000, 20
+    G = gw.Graph.rmat(scale, args.edge_factor, seed=args.graph_seed,
+                      blocksize_kb=blocksize_kb_for(scale, args.edge_factor, 16))
+    nv = G.nv
+    # "vertex 0" of the R-MAT generator (all-zero quadrant bits: its hub) is
+    # the vertex with the largest out-degree once ids are permuted
+    rp, _ = G.export_csr()
+    src = int(np.argmax(np.diff(rp.astype(np.int64))))
+    del rp
+    j = torch.arange(B, dtype=torch.int64, device="cuda")
+    walks = torch.stack([torch.full_like(j, src), j, torch.full_like(j, src), torch.zeros_like(j)], 1)
+    walks = walks.to(torch.int32).contiguous()
+    counts = torch.zeros(nv, dtype=torch.int32, device="cuda")
+    p = gw.params(gw.RULE_PPR, gw.SINK_VERTEX_COUNT, L, seed=args.walk_seed, aggregate=True)
+    sh = torch.cuda.current_stream().cuda_stream
+    for _ in range(max(3, args.warmup)):
+        counts.zero_()
+        G.walk_device(p, walks, B, counts=counts, stream=sh)
+    G.sync(sh)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for a, b in ev:
+        counts.zero_()
+        a.record()
+        G.walk_device(p, walks, B, counts=counts, stream=sh)
+        b.record()
+    G.sync(sh)
+    ms = statistics.median(a.elapsed_time(b) for a, b in ev)
+    c = counts.cpu().numpy().view(np.uint32).astype(np.float64)
+    steps = int(c.sum())
+    ids, cnt, st = G.ppr(p, np.array([src], np.uint32), np.array([B], np.uint32), k=100)
+    # accuracy against the FP64 power series of the same walk semantics
+    mu = G.expected_visits(p, src)
+    est = c / B
+    l1 = float(np.abs(est - mu).sum())
+    bound = float(np.sqrt(L * mu / B).sum())
+    exact_top = set(np.argsort(-mu, kind="stable")[:100].tolist())
+    overlap = len(exact_top & set(ids[0].tolist()))
+    top_from_counts = np.lexsort((np.arange(nv), -c))[:100]
+    top_from_counts = np.where(c[top_from_counts] > 0, top_from_counts, 0xFFFFFFFF)
+    line = {"metric": "walk-steps/s", "value": steps / (ms * 1e-3), "unit": "walk-steps/s", "workload": "ppr1",
+            "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": f"single-source PPR, R-MAT scale {scale} ef {args.edge_factor}, {B} walks from "
+                                   f"the generator's vertex 0 (id {src} after permutation, the top out-degree "
+                                   f"vertex), stop p=0.15, dangling->source, L<=20", "walk_steps": steps},
+            "queries_per_s": 1e3 / ms, "ppr_api_ms": st.ms_total,
+            "accuracy": {"l1_error": l1, "mc_bound_l1": bound, "top100_overlap_with_fp64": overlap,
+                         "top100_api_equals_counts": bool(np.array_equal(ids[0], top_from_counts))}}
+    G.close()
+    print(json.dumps(line), flush=True)
+
+
+def ooc_arm(args) -> None:
+    """Out-of-core raw random walks: the CSR held in pinned host memory as 256
+    blocks, streamed into a bounded number of device block slots by the
+    blocked engine (state-aware scheduling, double-buffered copies on a side
+    stream); one walk per vertex, L = 10, 64-bit walk state resident."""
+    import numpy as np
+    import torch
+
+    import graphwalker_b200 as gw
+    torch.cuda.set_device(0)
+    scale = args.scale if args.scale != 24 else 27
+    ef = args.edge_factor if args.edge_factor != 16 else 48
+    nblocks = args.nblocks if args.nblocks != 32 else 256
+    kb = blocksize_kb_for(scale, ef, nblocks)
+    t0 = time.perf_counter()
+    G = gw.Graph.rmat(scale, ef, seed=args.graph_seed, blocksize_kb=kb)
+    gen_s = time.perf_counter() - t0
+    nv, L = G.nv, args.L
+    graph_bytes = (nv + 1) * 8 + G.ne * 4
+    cur = np.arange(nv, dtype=np.uint32)
+    res = {}
+    # the same walks three ways: one resident launch, the resident block loop, streamed blocks
+    G.walks_clear()
+    G.add_walks_at(cur)
+    del cur
+    for name, residency, mode in (("resident_one_launch", gw.RESIDENT_HBM, gw.MODE_RESIDENT),
+                                  ("resident_blocked", gw.RESIDENT_HBM, gw.MODE_BLOCKED),
+                                  ("streamed_blocked", gw.STREAM_PINNED, gw.MODE_BLOCKED)):
+        G.set_residency(residency, nmblocks=args.nmblocks)
+        st = G.run(gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, L, seed=args.walk_seed, mode=mode, prob=0.2))
+        total = int(G.read_counts().astype(np.int64).sum())
+        if total != nv * L:
+            raise RuntimeError(f"{name}: {total} visits, expected {nv * L}")
+        res[name] = {"ms": st.ms_total, "walk_steps_per_s": nv * L / (st.ms_total * 1e-3),
+                     "supersteps": int(st.supersteps), "block_loads": int(st.block_loads),
+                     "h2d_GB": st.bytes_h2d / 1e9,
+                     "h2d_GBps": st.bytes_h2d / (st.ms_total * 1e-3) / 1e9 if st.bytes_h2d else 0.0}
+        print(json.dumps({name: res[name]}), flush=True)
+    s = res["streamed_blocked"]
+    line = {"metric": "walk-steps/s", "value": s["walk_steps_per_s"], "unit": "walk-steps/s", "workload": "ooc",
+            "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": s["ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": f"out-of-core raw random walks, R-MAT scale {scale} ef {ef}, {G.nblocks} blocks in "
+                                   f"pinned host memory, {args.nmblocks} device block slots, one walk per vertex, "
+                                   f"L={L}, jump rule", "graph_GB": graph_bytes / 1e9, "generate_s": gen_s},
+            "modes": res}
+    G.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.workload == "ooc" and args.impl != "reference":
+        ooc_arm(args)
+        return
+    if args.workload == "ppr1" and args.impl != "reference":
+        ppr1_arm(args)
+        return
     if args.impl == "reference":
         reference_arm(args)
     elif args.workload == "msppr":

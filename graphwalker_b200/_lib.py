@@ -56,7 +56,8 @@ class ServeStats(Structure):
 
 class PprStats(Structure):
     _fields_ = [("walks", c_uint64), ("table_slots", c_uint64), ("launches", c_uint32), ("reserved", c_uint32),
-                ("ms_clear", c_double), ("ms_walk", c_double), ("ms_topk", c_double), ("ms_total", c_double)]
+                ("ms_clear", c_double), ("ms_walk", c_double), ("ms_topk", c_double), ("ms_total", c_double),
+                ("visits", c_uint64)]
 
 
 HINT_EXPLICIT = 0x80000000
@@ -101,6 +102,7 @@ _SIGS = {
     "gw_graph_info": (c_int32, [_P, POINTER(c_uint32), POINTER(c_uint64), POINTER(c_uint32)]),
     "gw_get_blocks": (c_int32, [_P, _P, c_uint32]),
     "gw_export_csr": (c_int32, [_P, _P, _P]),
+    "gw_set_residency": (c_int32, [_P, c_uint32, c_uint32]),
     "gw_walks_clear": (c_int32, [_P]),
     "gw_walks_add": (c_int32, [_P, c_uint32, _P, _P, c_size_t]),
     "gw_walks_count": (c_int32, [_P, _P, POINTER(c_uint64)]),
@@ -120,6 +122,7 @@ _SIGS = {
     "gw_ppr_run": (c_int32, [_P, POINTER(WalkParams), _P, _P, c_uint32, c_uint32, c_uint32, _P, _P,
                              POINTER(PprStats)]),
     "gw_ppr_autotune": (c_int32, [_P, POINTER(WalkParams), _P, _P, c_uint32, POINTER(c_uint32)]),
+    "gw_expected_visits": (c_int32, [_P, POINTER(WalkParams), c_uint32, _P]),
     "gw_serve_open": (c_int32, [_P, POINTER(WalkParams), POINTER(ServeConfig), POINTER(c_void_p)]),
     "gw_serve_submit": (c_int32, [_P, c_uint32, c_uint32, c_uint32, c_uint64, POINTER(c_uint64)]),
     "gw_serve_wait": (c_int32, [_P, c_uint64, ctypes.c_int64, _P, _P, POINTER(ServeTiming)]),

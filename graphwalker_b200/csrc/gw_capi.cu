@@ -399,7 +399,7 @@ gw_status gw_close(gw_ctx* ctx) {
                        &ctx->d_tile_hist, &ctx->d_tile_off, &ctx->d_totals, &ctx->d_minhop,
                        &ctx->d_scan_temp, &ctx->d_out_ptr, &ctx->d_out_base, &ctx->d_q_sources,
                        &ctx->d_q_prefix, &ctx->d_q_idbase, &ctx->d_q_toff, &ctx->d_q_tmask, &ctx->d_q_tables,
-                       &ctx->d_q_full, &ctx->d_q_ids, &ctx->d_q_counts})
+                       &ctx->d_q_full, &ctx->d_q_ids, &ctx->d_q_counts, &ctx->d_q_visits})
     b->release();
   for (gw_devbuf& b : ctx->pools) b.release();
   ctx->h_rowptr.release();
@@ -439,6 +439,37 @@ gw_status gw_export_csr(gw_ctx* ctx, uint64_t* rowptr, uint32_t* colidx) {
   GW_CUDA(ctx, cudaMemcpy(rowptr, ctx->d_rowptr.p, rp, cudaMemcpyDeviceToHost), "rowptr export");
   if (colidx && ci)
     GW_CUDA(ctx, cudaMemcpy(colidx, ctx->d_colidx.p, ci, cudaMemcpyDeviceToHost), "colidx export");
+  return GW_OK;
+}
+
+gw_status gw_set_residency(gw_ctx* ctx, uint32_t residency, uint32_t nmblocks) {
+  if (!ctx) return set_thread_error(GW_E_INVALID, "NULL context");
+  if (residency > GW_STREAM_PINNED) return ctx->fail(GW_E_INVALID, "unknown residency %u", residency);
+  if (nmblocks) ctx->nmblocks = nmblocks;
+  if (residency == ctx->residency) return GW_OK;
+  const size_t rp = ((size_t)ctx->nv + 1) * 8, ci = (size_t)ctx->ne * 4;
+  GW_CUDA(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (residency == GW_STREAM_PINNED) {
+    GW_CUDA(ctx, ctx->h_rowptr.ensure(rp), "pinned rowptr");
+    GW_CUDA(ctx, ctx->h_colidx.ensure(ci), "pinned colidx");
+    GW_CUDA(ctx, cudaMemcpy(ctx->h_rowptr.p, ctx->d_rowptr.p, rp, cudaMemcpyDeviceToHost), "rowptr to host");
+    if (ci) GW_CUDA(ctx, cudaMemcpy(ctx->h_colidx.p, ctx->d_colidx.p, ci, cudaMemcpyDeviceToHost), "colidx to host");
+    ctx->d_rowptr.release();
+    ctx->d_colidx.release();
+    ctx->d_vrec.release();
+  } else {
+    GW_CUDA(ctx, ctx->d_rowptr.ensure(rp), "rowptr alloc");
+    GW_CUDA(ctx, ctx->d_colidx.ensure(ci), "colidx alloc");
+    GW_CUDA(ctx, ctx->d_vrec.ensure((size_t)ctx->nv * 8), "vrec alloc");
+    GW_CUDA(ctx, cudaMemcpy(ctx->d_rowptr.p, ctx->h_rowptr.p, rp, cudaMemcpyHostToDevice), "rowptr to device");
+    if (ci) GW_CUDA(ctx, cudaMemcpy(ctx->d_colidx.p, ctx->h_colidx.p, ci, cudaMemcpyHostToDevice), "colidx to device");
+    GW_CUDA(ctx, gw::launch_build_vrec(ctx->d_rowptr.as<unsigned long long>(), ctx->nv,
+                                       ctx->d_vrec.as<unsigned long long>(), ctx->stream), "build_vrec");
+    GW_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    ctx->h_rowptr.release();
+    ctx->h_colidx.release();
+  }
+  ctx->residency = residency;
   return GW_OK;
 }
 
@@ -726,6 +757,10 @@ gw_status gw_set_l2_persisting(gw_ctx* ctx, uint64_t bytes) {
   int max_persist = 0;
   GW_CUDA(ctx, cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, ctx->device),
           "max persisting L2");
+  int max_window = 0;
+  GW_CUDA(ctx, cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, ctx->device),
+          "max access policy window");
+  ctx->max_window_bytes = (size_t)std::max(max_window, 0);
   const uint64_t b = std::min<uint64_t>(bytes, (uint64_t)max_persist);
   GW_CUDA(ctx, cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, (size_t)b), "persisting L2 limit");
   if (b == 0) GW_CUDA(ctx, cudaCtxResetPersistingL2Cache(), "reset persisting L2");

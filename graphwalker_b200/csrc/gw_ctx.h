@@ -100,15 +100,19 @@ struct gw_ctx {
 
   // multi-source PPR queries
   gw_devbuf d_q_sources, d_q_prefix, d_q_idbase, d_q_toff, d_q_tmask, d_q_tables, d_q_full, d_q_ids,
-      d_q_counts;
+      d_q_counts, d_q_visits;
   int ppr_threads_per_sm = 0;  // autotuned launch shape (0 = full occupancy)
 
   std::string err;
 
-  // Access policy window over `counts` when an L2 reservation is active.
+  size_t max_window_bytes = 0;  // cudaDevAttrMaxAccessPolicyWindowSize
+
+  // Access policy window over `counts` when an L2 reservation is active
+  // (the window covers at most the device's maximum window size).
   bool counts_window(const void* counts, cudaAccessPolicyWindow* w) const {
-    if (!l2_persist_bytes || !counts) return false;
-    const size_t bytes = (size_t)nv * sizeof(uint32_t);
+    if (!l2_persist_bytes || !counts || !max_window_bytes) return false;
+    size_t bytes = (size_t)nv * sizeof(uint32_t);
+    if (bytes > max_window_bytes) bytes = max_window_bytes;
     w->base_ptr = const_cast<void*>(counts);
     w->num_bytes = bytes;
     w->hitRatio = bytes <= l2_persist_bytes ? 1.0f : (float)l2_persist_bytes / (float)bytes;

@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(kPprThreads)
   // stream id = the walk's position in the original batch
   unsigned long long id_shift = qv.id_base ? __ldg(qv.id_base + q) - __ldg(qv.walk_prefix + q) : 0ull;
   uint32_t sid = qv.stream ? __ldg(qv.stream + q) : 0u;
-  uint32_t v = src, hop = 0, st = 0;
+  uint32_t v = src, hop = 0, st = 0, nvisit = 0;
   for (;;) {
     bool end;
     if (rule_capped<RULE>() && hop >= a.L) {
@@ -93,6 +93,7 @@ __global__ void __launch_bounds__(kPprThreads)
     } else {
       // the record load is issued before the table update so the two overlap
       const unsigned long long rec = ld_nc_u64(g.vrec + v, hp.rec);
+      ++nvisit;
       // fold lanes visiting the same (query, vertex) into one update
       const unsigned active = __activemask();
       const unsigned long long key = ((unsigned long long)q << 32) | v;
@@ -121,6 +122,11 @@ __global__ void __launch_bounds__(kPprThreads)
     }
   }
   if (st) atomicOr(status, st);
+  if (qv.visits) {
+    const unsigned m = __activemask();
+    const unsigned long long w = __reduce_add_sync(m, nvisit);
+    if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(qv.visits, w);
+  }
 }
 
 // Sorts keys[0, n) in shared memory, largest first (bitonic; n a power of two).

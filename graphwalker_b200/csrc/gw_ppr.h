@@ -19,6 +19,7 @@ struct QueryView {
   unsigned long long* tables;              // all tables, slots (vertex << 32 | count), ~0 = empty
   uint32_t* full;                          // nq: set to 1 when query q's table filled up
   const uint32_t* stream;                  // nq: Philox stream word of query q (NULL = 0)
+  unsigned long long* visits;              // total visits counter (may be NULL)
   uint32_t nq;
 };
 

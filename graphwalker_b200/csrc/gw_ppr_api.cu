@@ -161,6 +161,8 @@ extern "C" gw_status gw_ppr_run(gw_ctx* ctx, const gw_walk_params* params, const
   for (uint32_t q = 0; q < nq; ++q) which[q] = q;
   uint64_t factor = params->table_factor ? params->table_factor : 8;
   cudaStream_t st = ctx->stream;
+  GW_CUDA(ctx, ctx->d_q_visits.ensure(8), "visit counter");
+  GW_CUDA(ctx, cudaMemsetAsync(ctx->d_q_visits.p, 0, 8, st), "visit counter");
   cudaEvent_t ev[4];
   for (auto& e : ev) cudaEventCreate(&e);
   gw_ppr_stats local{};
@@ -171,6 +173,7 @@ extern "C" gw_status gw_ppr_run(gw_ctx* ctx, const gw_walk_params* params, const
     s = plan_set(ctx, sources, budgets, ids.data(), which, factor, &set);
     if (s == GW_OK) s = upload_set(ctx, &set, k, st);
     if (s != GW_OK) break;
+    set.qv.visits = ctx->d_q_visits.as<unsigned long long>();
     const bool b = batched || round > 0;
     cudaError_t e = run_set(ctx, params, a, &set, k, b, b ? ctx->ppr_threads_per_sm : 0, st, ev, &local.launches);
     const uint32_t n = (uint32_t)which.size();
@@ -207,6 +210,8 @@ extern "C" gw_status gw_ppr_run(gw_ctx* ctx, const gw_walk_params* params, const
     factor *= 4;
   }
   for (auto& x : ev) cudaEventDestroy(x);
+  unsigned long long nvis = 0;
+  if (cudaMemcpy(&nvis, ctx->d_q_visits.p, 8, cudaMemcpyDeviceToHost) == cudaSuccess) local.visits = nvis;
   if (s == GW_OK && !which.empty())
     s = ctx->fail(GW_E_OVERFLOW, "%zu queries still filled their visit tables after %d retries",
                   which.size(), kMaxRetries);

@@ -143,6 +143,10 @@ class Graph:
         check(load().gw_export_csr(self._h, _ptr(rowptr), _ptr(colidx)), self._h)
         return rowptr, colidx[: self.ne]
 
+    def set_residency(self, residency: int, nmblocks: int = 0) -> None:
+        """Moves the CSR between HBM and pinned host memory (streamed blocks)."""
+        check(load().gw_set_residency(self._h, residency, nmblocks), self._h)
+
     # ---- pools (WalkManager) ----
     def walks_clear(self) -> None:
         check(load().gw_walks_clear(self._h), self._h)
@@ -241,6 +245,12 @@ class Graph:
         check(load().gw_ppr_run(self._h, byref(p), _ptr(sources), _ptr(budgets), nq, k, int(batched), _ptr(ids),
                                 _ptr(counts), byref(st)), self._h)
         return ids.reshape(nq, k), counts.reshape(nq, k), st
+
+    def expected_visits(self, p: WalkParams, source: int) -> np.ndarray:
+        """FP64 expected visits per vertex of one walk from `source`."""
+        out = np.zeros(self.nv, dtype=np.float64)
+        check(load().gw_expected_visits(self._h, byref(p), source, _ptr(out)), self._h)
+        return out
 
     def ppr_autotune(self, p: WalkParams, sources, budgets) -> int:
         sources = np.ascontiguousarray(sources, dtype=np.uint32)

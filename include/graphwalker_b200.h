@@ -161,6 +161,10 @@ gw_status gw_graph_info(gw_ctx *ctx, uint32_t *nvertices, uint64_t *nedges, uint
 gw_status gw_get_blocks(gw_ctx *ctx, uint32_t *blocks, uint32_t cap);
 /* Copies the CSR to host buffers (rowptr: nvertices+1, colidx: nedges).     */
 gw_status gw_export_csr(gw_ctx *ctx, uint64_t *rowptr, uint32_t *colidx);
+/* Moves the CSR between HBM (GW_RESIDENT_HBM) and pinned host memory
+   (GW_STREAM_PINNED, blocks streamed into `nmblocks` device slots, the
+   reference's in-memory block budget, graphwalker.hpp:84-86).              */
+gw_status gw_set_residency(gw_ctx *ctx, uint32_t residency, uint32_t nmblocks);
 
 /* ---- walk pools (WalkManager) ------------------------------------------- */
 gw_status gw_walks_clear(gw_ctx *ctx);
@@ -202,6 +206,7 @@ typedef struct gw_ppr_stats {
   double ms_walk;        /* device time of the walk kernels                    */
   double ms_topk;        /* device time of the top-k kernels                   */
   double ms_total;       /* device time of the whole call (first to last op)   */
+  uint64_t visits;       /* walk steps (visits) run, re-runs of full tables too */
 } gw_ppr_stats;
 
 /* Runs budgets[q] walks from sources[q] for each of nq queries with the
@@ -217,6 +222,10 @@ typedef struct gw_ppr_stats {
 gw_status gw_ppr_run(gw_ctx *ctx, const gw_walk_params *params, const uint32_t *sources,
                      const uint32_t *budgets, uint32_t nq, uint32_t k, uint32_t batched,
                      uint32_t *topk_ids, uint32_t *topk_counts, gw_ppr_stats *stats);
+/* Exact expected visits per vertex of ONE walk from `source` under
+   params->rule / L / jump_prob, in FP64 (out[nvertices]): the truncated
+   power series the Monte Carlo counts estimate (count / walks -> out).      */
+gw_status gw_expected_visits(gw_ctx *ctx, const gw_walk_params *params, uint32_t source, double *out);
 /* Times candidate launch shapes of the batched query kernel on the given
    queries (a sample of the workload) and keeps the fastest for this
    context; *threads_per_sm receives the choice.                            */

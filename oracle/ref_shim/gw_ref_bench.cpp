@@ -2,28 +2,36 @@
  * gw_ref_bench.cpp -- BENCHMARK INFRASTRUCTURE (the CPU reference arm).
  *
  * Times GraphWalker's own CPU engine (src/engine/graphwalker.hpp) and walk
- * class, compiled unmodified from the reference tree with its native glibc
- * rand_r, on a preprocessed graph.  The app below mirrors
- * apps/rwdomination.cpp (RandomWalkwithJump, per-vertex visit counter
- * incremented without atomics in updateInfo, walks placed block by block
- * with source = start vertex) but starts one walk on every `stride`-th vertex
- * so that one engine run is a bounded sample of the one-walk-per-vertex
- * workload; the engine object (and its in-memory block cache) is reused
- * across runs, so runs after the first see the graph resident in RAM, as
- * the GPU engine sees it resident in HBM.
+ * classes, compiled unmodified from the reference tree with its native glibc
+ * rand_r, on a preprocessed graph.  The engine object (and its in-memory
+ * block cache) is reused across runs, so runs after the first see the graph
+ * resident in RAM, as the GPU engine sees it resident in HBM.
  *
- * Usage: gw_ref_bench <graph base> <blocksize_kb> <N> <L> <stride>
- *                     <warmup> <steps> <execthreads> [rule]
- *   rule 0 = RandomWalkwithJump (rwdomination), 1 = RandomWalkwithStop (msppr)
+ * Apps:
+ *   rwd   -- mirrors apps/rwdomination.cpp: RandomWalkwithJump, a per-vertex
+ *            visit counter incremented without atomics in updateInfo, walks
+ *            placed block by block with source = start vertex; one walk on
+ *            every `stride`-th vertex (a bounded sample of one walk per vertex).
+ *   msppr -- mirrors apps/msppr.cpp's placement (walkspersource walks on each
+ *            of `numsources` sources starting at firstsource, source field =
+ *            source index) with RandomWalkwithStop; the per-visit sink is a
+ *            per-thread counter as in apps/kk_ppr.cpp, because msppr's
+ *            DiscreteDistribution::add is not thread-safe.
+ *
+ * Usage: gw_ref_bench <graph base> <blocksize_kb> <N> <L> <stride> <warmup>
+ *                     <steps> <execthreads> [rwd | msppr <firstsource>
+ *                     <numsources> <walkspersource>]
  * Prints one line per timed run: "step <i> walks <n> steps <visits> sec <t>".
  */
 #include <chrono>
 #include <cmath>
 #include <fstream>
 #include <string>
+#include <vector>
 
 #include "api/graphwalker_basic_includes.hpp"
 #include "walks/randomwalkwithjump.hpp"
+#include "walks/randomwalkwithstop.hpp"
 
 class BenchDomination : public RandomWalkwithJump {
 public:
@@ -56,9 +64,56 @@ public:
     }
 };
 
+class BenchMsppr : public RandomWalkwithStop {
+public:
+    vid_t firstsource = 0, numsources = 1;
+    wid_t walkspersource = 1;
+    std::vector<unsigned long long> visits;  // per thread, padded
+    wid_t started = 0;
+
+    void startWalksbyApp(WalkManager &walk_manager) {
+        tid_t nthreads = get_option_int("execthreads", omp_get_max_threads());
+        omp_set_num_threads(nthreads);
+        visits.assign((size_t)nthreads * 16, 0);
+        // apps/msppr.cpp:41-69: sources block by block, source field = source index
+        bid_t p = getblock(firstsource);
+        vid_t sts = firstsource, ens = blocks[p + 1];
+        vid_t count = numsources;
+        walk_manager.walksum = 0;
+        while (count > 0) {
+            if (ens > firstsource + numsources) ens = firstsource + numsources;
+            vid_t nums = ens - sts;
+            count -= nums;
+            walk_manager.minstep[p] = 0;
+            walk_manager.walknum[p] = nums * walkspersource;
+#pragma omp parallel for schedule(static)
+            for (vid_t s = 0; s < nums; s++) {
+                vid_t cur = s + sts - blocks[p];
+                WalkDataType walk = walk_manager.encode(s + sts - firstsource, cur, 0);
+                for (wid_t j = 0; j < walkspersource; j++)
+                    walk_manager.moveWalk(walk, p, omp_get_thread_num(), cur);
+            }
+            walk_manager.walksum += walk_manager.walknum[p];
+            p++;
+            sts = ens;
+            ens = blocks[p + 1];
+        }
+        started = walk_manager.walksum;
+    }
+
+    void updateInfo(vid_t s, vid_t dstId, tid_t threadid, hid_t hop) { visits[(size_t)threadid * 16]++; }
+
+    unsigned long long total_visits() const {
+        unsigned long long t = 0;
+        for (size_t i = 0; i < visits.size(); i += 16) t += visits[i];
+        return t;
+    }
+};
+
 int main(int argc, const char **argv) {
     if (argc < 9) {
-        fprintf(stderr, "usage: %s graph blocksize_kb N L stride warmup steps execthreads\n", argv[0]);
+        fprintf(stderr, "usage: %s graph blocksize_kb N L stride warmup steps execthreads [rwd|msppr first num wps]\n",
+                argv[0]);
         return 2;
     }
     set_argc(argc, argv);
@@ -69,22 +124,41 @@ int main(int argc, const char **argv) {
     hid_t L = (hid_t)atoi(argv[4]);
     vid_t stride = (vid_t)strtoul(argv[5], nullptr, 10);
     int warmup = atoi(argv[6]), steps = atoi(argv[7]);
+    const std::string app = argc > 10 ? argv[10] : "rwd";
 
-    BenchDomination app;
-    app.initializeRW(N, 1, L);
-    app.stride = stride ? stride : 1;
-    app.vertex_value = new unsigned[N]();
     bid_t nblocks = convert_if_notexists(graph, blocksize_kb);
     graphwalker_engine engine(graph, blocksize_kb, nblocks, nblocks, m);
+    if (app == "msppr") {
+        if (argc < 14) return 2;
+        BenchMsppr prog;
+        prog.firstsource = (vid_t)strtoul(argv[11], nullptr, 10);
+        prog.numsources = (vid_t)strtoul(argv[12], nullptr, 10);
+        prog.walkspersource = strtoull(argv[13], nullptr, 10);
+        prog.initializeRW(prog.numsources * prog.walkspersource, L);
+        for (int i = 0; i < warmup + steps; ++i) {
+            auto t0 = std::chrono::steady_clock::now();
+            engine.run(prog, 0.2f);
+            auto t1 = std::chrono::steady_clock::now();
+            if (i >= warmup)
+                printf("step %d walks %llu steps %llu sec %.6f\n", i - warmup, (unsigned long long)prog.started,
+                       prog.total_visits(), std::chrono::duration<double>(t1 - t0).count());
+            fflush(stdout);
+        }
+        return 0;
+    }
+    BenchDomination prog;
+    prog.initializeRW(N, 1, L);
+    prog.stride = stride ? stride : 1;
+    prog.vertex_value = new unsigned[N]();
     for (int i = 0; i < warmup + steps; ++i) {
-        std::fill(app.vertex_value, app.vertex_value + N, 0u);
+        std::fill(prog.vertex_value, prog.vertex_value + N, 0u);
         auto t0 = std::chrono::steady_clock::now();
-        engine.run(app, 0.2f);
+        engine.run(prog, 0.2f);
         auto t1 = std::chrono::steady_clock::now();
         unsigned long long visits = 0;
-        for (vid_t v = 0; v < N; ++v) visits += app.vertex_value[v];
+        for (vid_t v = 0; v < N; ++v) visits += prog.vertex_value[v];
         if (i >= warmup)
-            printf("step %d walks %llu steps %llu sec %.6f\n", i - warmup, (unsigned long long)app.started,
+            printf("step %d walks %llu steps %llu sec %.6f\n", i - warmup, (unsigned long long)prog.started,
                    visits, std::chrono::duration<double>(t1 - t0).count());
         fflush(stdout);
     }

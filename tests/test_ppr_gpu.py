@@ -121,3 +121,15 @@ def test_ppr_accuracy_against_fp64_power_series(cuda_device, oracle):
         assert np.all(np.abs(est - mu[ids[q]]) <= 5 * sd + 1e-9)
         exact_top = set(np.argsort(-mu, kind="stable")[:100].tolist())
         assert len(exact_top & set(ids[q].tolist())) >= 90
+
+
+@pytest.mark.parametrize("rule,L", [(0, 10), (1, 20), (3, 7), (4, 20), (2, 0)])
+def test_expected_visits_kernel_matches_fp64_oracle(cuda_device, oracle, rule, L):
+    import graphwalker_b200 as gw
+    rp, ci = oracle.rmat_csr(12, 8, seed=17)
+    deg = np.diff(rp.astype(np.int64))
+    src = int(np.argmax(deg))
+    with gw.Graph.from_csr(rp, ci, oracle.compute_blocks(rp, 32)) as G:
+        got = G.expected_visits(gw.params(rule, gw.SINK_NONE, L), src)
+    ref = oracle.expected_visits(rp, ci, src, rule, L)
+    assert np.allclose(got, ref, rtol=1e-9, atol=1e-13)
