@@ -399,7 +399,8 @@ gw_status gw_close(gw_ctx* ctx) {
                        &ctx->d_tile_hist, &ctx->d_tile_off, &ctx->d_totals, &ctx->d_minhop,
                        &ctx->d_scan_temp, &ctx->d_out_ptr, &ctx->d_out_base, &ctx->d_q_sources,
                        &ctx->d_q_prefix, &ctx->d_q_idbase, &ctx->d_q_toff, &ctx->d_q_tmask, &ctx->d_q_tables,
-                       &ctx->d_q_full, &ctx->d_q_ids, &ctx->d_q_counts, &ctx->d_q_visits})
+                       &ctx->d_q_full, &ctx->d_q_ids, &ctx->d_q_counts, &ctx->d_q_visits,
+                       &ctx->d_q_cursor})
     b->release();
   for (gw_devbuf& b : ctx->pools) b.release();
   ctx->h_rowptr.release();

@@ -10,8 +10,10 @@
 // (vertex << 32 | count; all-ones = empty) -- the sparse replacement of
 // msppr's per-source DiscreteDistribution (discretedistribution.hpp:44-57).
 // Lanes of a warp that visit the same (query, vertex) in the same step are
-// folded into one table update (every walk of a query visits its source at
-// hop 0).
+// folded into one table update, and the hop-0 visits of a query's walks (all
+// at its source) are added in one update.  Warps take walks in small chunks
+// of consecutive batch positions from a global cursor, so the walks in flight
+// belong to a narrow window of queries whose tables stay in L2.
 //
 // Top-k: one CTA per query scans its table and keeps a candidate buffer of
 // keys (count << 32 | ~vertex): whenever the buffer could overflow it is
@@ -26,6 +28,13 @@ namespace {
 
 constexpr unsigned long long kEmptySlot = ~0ull;
 
+// Longest probe sequence an update walks before it reports the table full:
+// bounds the cost of a filling table (whose query is then rerun with a larger
+// one) instead of letting every further update scan the whole table.
+constexpr uint32_t kMaxProbes = 256;
+
+__device__ __forceinline__ uint32_t probe_limit(uint32_t mask) { return mask < kMaxProbes ? mask : kMaxProbes - 1; }
+
 __device__ __forceinline__ uint32_t slot_hash(uint32_t v) {  // MurmurHash3 fmix32 (Appleby)
   v ^= v >> 16;
   v *= 0x85ebca6bu;
@@ -35,24 +44,51 @@ __device__ __forceinline__ uint32_t slot_hash(uint32_t v) {  // MurmurHash3 fmix
   return v;
 }
 
-// Adds n visits of vertex v to a table; false when the table is full.
-__device__ __forceinline__ bool table_add(unsigned long long* __restrict__ t, uint32_t mask, uint32_t v,
-                                          uint32_t n) {
-  uint32_t s = slot_hash(v) & mask;
-  for (uint32_t probe = 0; probe <= mask; ++probe) {
-    unsigned long long* e = t + s;
-    unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(e);
-    if (cur == kEmptySlot) {
-      cur = atomicCAS(e, kEmptySlot, ((unsigned long long)v << 32) | n);
-      if (cur == kEmptySlot) return true;
-    }
-    if ((uint32_t)(cur >> 32) == v) {
-      atomicAdd(e, (unsigned long long)n);
+// Slot operations.  The add carries an L2 eviction policy (the tables of the
+// queries in flight should stay in L2 while the graph streams through it);
+// the compare-and-swap form of atom takes none.
+__device__ __forceinline__ unsigned long long cas_u64(unsigned long long* a, unsigned long long cmp,
+                                                      unsigned long long val) {
+  unsigned long long old;
+  asm volatile("atom.relaxed.gpu.global.cas.b64 %0, [%1], %2, %3;" : "=l"(old) : "l"(a), "l"(cmp), "l"(val)
+               : "memory");
+  return old;
+}
+
+__device__ __forceinline__ void red_add_u64(unsigned long long* a, unsigned long long v, uint64_t pol) {
+  asm volatile("red.relaxed.gpu.global.add.L2::cache_hint.u64 [%0], %1, %2;" ::"l"(a), "l"(v), "l"(pol)
+               : "memory");
+}
+
+// Completes a table update whose first probe (a CAS at slot s) returned
+// `old`: nothing to do if the CAS claimed the slot, an add if the slot holds
+// v, otherwise linear probing from s + 1.  False when the table is full (no
+// free slot or slot holding v within kMaxProbes of s).
+__device__ __forceinline__ bool table_finish(unsigned long long* __restrict__ t, uint32_t mask, uint32_t s,
+                                             unsigned long long old, uint32_t v, uint32_t n, uint64_t pol) {
+  if (old == kEmptySlot) return true;
+  if ((uint32_t)(old >> 32) == v) {
+    red_add_u64(t + s, n, pol);
+    return true;
+  }
+  const uint32_t last = probe_limit(mask);
+  for (uint32_t probe = 1; probe <= last; ++probe) {
+    s = (s + 1) & mask;
+    old = cas_u64(t + s, kEmptySlot, ((unsigned long long)v << 32) | n);
+    if (old == kEmptySlot) return true;
+    if ((uint32_t)(old >> 32) == v) {
+      red_add_u64(t + s, n, pol);
       return true;
     }
-    s = (s + 1) & mask;
   }
   return false;
+}
+
+// Adds n visits of vertex v to a table; false when the table is full.
+__device__ __forceinline__ bool table_add(unsigned long long* __restrict__ t, uint32_t mask, uint32_t v,
+                                          uint32_t n, uint64_t pol) {
+  const uint32_t s = slot_hash(v) & mask;
+  return table_finish(t, mask, s, cas_u64(t + s, kEmptySlot, ((unsigned long long)v << 32) | n), v, n, pol);
 }
 
 __device__ __forceinline__ uint32_t query_of(const unsigned long long* __restrict__ prefix, uint32_t nq,
@@ -70,17 +106,61 @@ template <int RULE>
 __global__ void __launch_bounds__(kPprThreads)
     walk_query_kernel(QueryView qv, unsigned long long w_begin, unsigned long long w_end, GraphView g,
                       WalkArgs a, uint32_t* __restrict__ status) {
-  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-  unsigned long long j = w_begin + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= w_end) return;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t below = (1u << lane) - 1u;  // lanes under this one
+  const unsigned long long total = w_end - w_begin;
   const L2Hints hp = make_hints(a.hints);
-  uint32_t q = query_of(qv.walk_prefix, qv.nq, j);
-  uint32_t src = __ldg(qv.sources + q);
-  // stream id = the walk's position in the original batch
-  unsigned long long id_shift = qv.id_base ? __ldg(qv.id_base + q) - __ldg(qv.walk_prefix + q) : 0ull;
-  uint32_t sid = qv.stream ? __ldg(qv.stream + q) : 0u;
-  uint32_t v = src, hop = 0, st = 0, nvisit = 0;
+  // Every walk visits its source at hop 0: the first walk of each query in
+  // this launch adds all of them at once and the walks skip that update.
+  const bool visits_source =
+      !(rule_capped<RULE>() && a.L == 0) && !(RULE == GW_RULE_PROB && a.max_hops == 0);
+  unsigned long long c_next = 0, c_end = 0;  // the warp's current chunk of batch positions
+  bool drained = false;                      // the cursor has run past the batch (warp-uniform)
+  bool busy = false;                         // this lane holds a walk
+  unsigned long long j = 0, id_shift = 0, q_lo = 1, q_hi = 0;
+  uint32_t q = 0, src = 0, sid = 0, v = 0, hop = 0, st = 0, nvisit = 0;
   for (;;) {
+    // Idle lanes take the next walks of the warp's chunk, in lane order.
+    uint32_t idle = __ballot_sync(~0u, !busy);
+    while (idle && !drained) {
+      if (c_next >= c_end) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(qv.cursor, (unsigned long long)kWarpChunk);
+        base = __shfl_sync(~0u, base, 0);
+        if (base >= total) {
+          drained = true;
+          break;
+        }
+        c_next = base;
+        c_end = base + kWarpChunk < total ? base + kWarpChunk : total;
+      }
+      const unsigned long long avail = c_end - c_next;
+      if (!busy && __popc(idle & below) < avail) {
+        j = w_begin + c_next + __popc(idle & below);
+        busy = true;
+        if (j < q_lo || j >= q_hi) {
+          q = query_of(qv.walk_prefix, qv.nq, j);
+          q_lo = __ldg(qv.walk_prefix + q);
+          q_hi = __ldg(qv.walk_prefix + q + 1);
+          src = __ldg(qv.sources + q);
+          // stream id = the walk's position in the original batch
+          id_shift = qv.id_base ? __ldg(qv.id_base + q) - q_lo : 0ull;
+          sid = qv.stream ? __ldg(qv.stream + q) : 0u;
+        }
+        const unsigned long long lo = q_lo > w_begin ? q_lo : w_begin, hi = q_hi < w_end ? q_hi : w_end;
+        if (visits_source && j == lo && src < g.nv &&
+            !table_add(qv.tables + __ldg(qv.table_off + q), __ldg(qv.table_mask + q), src, (uint32_t)(hi - lo),
+                       hp.cnt))
+          qv.full[q] = 1u;
+        v = src;
+        hop = 0;
+      }
+      const uint32_t n_idle = __popc(idle);
+      c_next += n_idle < avail ? n_idle : avail;
+      idle = __ballot_sync(~0u, !busy);
+    }
+    if (!__any_sync(~0u, busy)) break;
+    if (!busy) continue;
     bool end;
     if (rule_capped<RULE>() && hop >= a.L) {
       end = true;
@@ -91,41 +171,62 @@ __global__ void __launch_bounds__(kPprThreads)
       st |= kStBounds;
       end = true;
     } else {
-      // the record load is issued before the table update so the two overlap
       const unsigned long long rec = ld_nc_u64(g.vrec + v, hp.rec);
       ++nvisit;
-      // fold lanes visiting the same (query, vertex) into one update
-      const unsigned active = __activemask();
-      const unsigned long long key = ((unsigned long long)q << 32) | v;
-      const unsigned peers = __match_any_sync(active, key);
-      if ((threadIdx.x & 31) == __ffs(peers) - 1) {
-        unsigned long long* t = qv.tables + __ldg(qv.table_off + q);
-        if (!table_add(t, __ldg(qv.table_mask + q), v, (uint32_t)__popc(peers))) qv.full[q] = 1u;
+      // Table update for hops >= 1: lanes visiting the same (query, vertex)
+      // fold into one; its first probe (a CAS) is issued now and resolved
+      // only after this hop's column load is in flight.
+      bool leader = false;
+      uint32_t n = 0, s0 = 0, mask = 0;
+      unsigned long long old = kEmptySlot, *t = nullptr;
+      if (hop > 0) {
+        const unsigned active = __activemask();
+        const unsigned peers = __match_any_sync(active, ((unsigned long long)q << 32) | v);
+        leader = lane == (uint32_t)__ffs(peers) - 1;
+        if (leader) {
+          n = (uint32_t)__popc(peers);
+          t = qv.tables + __ldg(qv.table_off + q);
+          mask = __ldg(qv.table_mask + q);
+          s0 = slot_hash(v) & mask;
+          old = cas_u64(t + s0, kEmptySlot, ((unsigned long long)v << 32) | n);
+        }
       }
-      end = !hop_advance_rec<RULE>(g, a, hp, (uint32_t)(j + id_shift), src, hop, v, rec, sid);
-      if (!end) {
+      // the hop itself: hop_advance_rec's draws and choices, written out so
+      // the table update above can complete after the column load is issued
+      const Philox4 ph = philox4x32_10((uint32_t)(j + id_shift), hop, sid, 0u, a.seed_lo, a.seed_hi);
+      const uint32_t d0 = ph.x >> 1, d1 = ph.y >> 1;
+      unsigned long long off = rec >> kDegBits, deg = rec & kDegEscape;
+      if (deg == kDegEscape) {
+        off = __ldg(g.rowptr + v);
+        deg = __ldg(g.rowptr + v + 1) - off;
+      }
+      uint32_t next = v;
+      bool moved = true;
+      if (deg > 0 && d0 >= a.thr) {
+        const unsigned long long r =
+            deg > 0x7fffffffull ? (unsigned long long)d1 : (unsigned long long)(d1 % (uint32_t)deg);
+        next = ld_nc_u32(g.colidx + off + r, hp.col);
+      } else {
+        const uint32_t dj = deg > 0 ? d1 : d0;
+        if (RULE == GW_RULE_JUMP) next = dj % a.njump;
+        else if (RULE == GW_RULE_RESTART) next = src;
+        else if (RULE == GW_RULE_PPR && deg == 0) next = src;
+        else moved = false;
+      }
+      if (leader && !table_finish(t, mask, s0, old, v, n, hp.cnt)) qv.full[q] = 1u;
+      end = !moved;
+      if (moved) {
+        v = next;
         ++hop;
         if (RULE == GW_RULE_RESTART && hop % a.L == a.L - 1) end = true;
       }
     }
-    if (end) {
-      j += stride;
-      if (j >= w_end) break;
-      if (j >= __ldg(qv.walk_prefix + q + 1)) {
-        q = query_of(qv.walk_prefix, qv.nq, j);
-        src = __ldg(qv.sources + q);
-        id_shift = qv.id_base ? __ldg(qv.id_base + q) - __ldg(qv.walk_prefix + q) : 0ull;
-        sid = qv.stream ? __ldg(qv.stream + q) : 0u;
-      }
-      v = src;
-      hop = 0;
-    }
+    if (end) busy = false;
   }
   if (st) atomicOr(status, st);
   if (qv.visits) {
-    const unsigned m = __activemask();
-    const unsigned long long w = __reduce_add_sync(m, nvisit);
-    if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(qv.visits, w);
+    const unsigned long long w = __reduce_add_sync(~0u, nvisit);
+    if (lane == 0 && w) atomicAdd(qv.visits, w);
   }
 }
 
@@ -164,27 +265,36 @@ __global__ void __launch_bounds__(kTopkThreads)
     thresh = 0;
   }
   __syncthreads();
-  for (uint32_t base = 0; base < cap; base += blockDim.x) {
-    const uint32_t i = base + threadIdx.x;
-    if (i < cap) {
-      const unsigned long long e = t[i];
-      if (e != kEmptySlot) {
-        const unsigned long long key = ((e & 0xffffffffull) << 32) | (uint32_t)~(uint32_t)(e >> 32);
+  // kTopkUnroll slots per thread are loaded together (so a large table is
+  // read with that many loads in flight per thread), then filtered one round
+  // of blockDim.x slots at a time.
+  const uint64_t pol = l2_policy(true, false);
+  for (uint32_t base = 0; base < cap; base += blockDim.x * kTopkUnroll) {
+    unsigned long long e[kTopkUnroll];
+#pragma unroll
+    for (uint32_t u = 0; u < kTopkUnroll; ++u) {
+      const uint32_t i = base + u * blockDim.x + threadIdx.x;
+      e[u] = i < cap ? ld_nc_u64(t + i, pol) : kEmptySlot;
+    }
+#pragma unroll
+    for (uint32_t u = 0; u < kTopkUnroll; ++u) {
+      if (e[u] != kEmptySlot) {
+        const unsigned long long key = ((e[u] & 0xffffffffull) << 32) | (uint32_t)~(uint32_t)(e[u] >> 32);
         if (key > thresh) {
           const uint32_t pos = atomicAdd(&ncand, 1u);
           cand[pos] = key;  // room for one full round is kept free below
         }
       }
-    }
-    __syncthreads();
-    if (ncand > kTopkBuffer - blockDim.x) {  // cut to the best k before the next round
-      for (uint32_t x = ncand + threadIdx.x; x < kTopkBuffer; x += blockDim.x) cand[x] = 0;
-      block_sort_desc(cand, kTopkBuffer);
-      if (threadIdx.x == 0) {
-        ncand = k;
-        thresh = cand[k - 1];
-      }
       __syncthreads();
+      if (ncand > kTopkBuffer - blockDim.x) {  // cut to the best k before the next round
+        for (uint32_t x = ncand + threadIdx.x; x < kTopkBuffer; x += blockDim.x) cand[x] = 0;
+        block_sort_desc(cand, kTopkBuffer);
+        if (threadIdx.x == 0) {
+          ncand = k;
+          thresh = cand[k - 1];
+        }
+        __syncthreads();
+      }
     }
   }
   for (uint32_t x = ncand + threadIdx.x; x < kTopkBuffer; x += blockDim.x) cand[x] = 0;
@@ -196,6 +306,20 @@ __global__ void __launch_bounds__(kTopkThreads)
   }
 }
 
+__global__ void clear_tables_kernel(ulonglong2* __restrict__ t, unsigned long long n2) {
+  const ulonglong2 empty = make_ulonglong2(kEmptySlot, kEmptySlot);
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n2;
+       i += (unsigned long long)gridDim.x * blockDim.x)
+    t[i] = empty;
+}
+
+int sm_count() {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
 template <int RULE>
 cudaError_t query_dispatch(const QueryView& qv, unsigned long long w_begin, unsigned long long w_end,
                            const GraphView& g, const WalkArgs& a, uint32_t* status, int threads_per_sm,
@@ -203,9 +327,7 @@ cudaError_t query_dispatch(const QueryView& qv, unsigned long long w_begin, unsi
   auto kern = walk_query_kernel<RULE>;
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPprThreads, 0);
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int sms = sm_count();
   if (per_sm <= 0) per_sm = 1;
   if (threads_per_sm > 0) per_sm = std::max(1, std::min(per_sm, threads_per_sm / kPprThreads));
   const unsigned long long n = w_end - w_begin;
@@ -222,6 +344,9 @@ cudaError_t launch_walk_queries(int rule, const QueryView& qv, unsigned long lon
                                 unsigned long long w_end, const GraphView& g, const WalkArgs& a,
                                 uint32_t* status, int threads_per_sm, cudaStream_t stream) {
   if (w_end <= w_begin || qv.nq == 0) return cudaSuccess;
+  if (!qv.cursor) return cudaErrorInvalidValue;
+  const cudaError_t e = cudaMemsetAsync(qv.cursor, 0, sizeof(unsigned long long), stream);
+  if (e != cudaSuccess) return e;
   switch (rule) {
     case GW_RULE_JUMP: return query_dispatch<GW_RULE_JUMP>(qv, w_begin, w_end, g, a, status, threads_per_sm, stream);
     case GW_RULE_STOP: return query_dispatch<GW_RULE_STOP>(qv, w_begin, w_end, g, a, status, threads_per_sm, stream);
@@ -231,6 +356,16 @@ cudaError_t launch_walk_queries(int rule, const QueryView& qv, unsigned long lon
     case GW_RULE_PPR: return query_dispatch<GW_RULE_PPR>(qv, w_begin, w_end, g, a, status, threads_per_sm, stream);
   }
   return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_clear_tables(unsigned long long* tables, unsigned long long n, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  if ((reinterpret_cast<uintptr_t>(tables) & 15) || (n & 1))  // not in 16-byte pairs: byte fill
+    return cudaMemsetAsync(tables, 0xff, n * sizeof(unsigned long long), stream);
+  const unsigned long long n2 = n / 2, need = (n2 + 255) / 256, full = (unsigned long long)sm_count() * 8;
+  clear_tables_kernel<<<(unsigned)(need < full ? need : full), 256, 0, stream>>>(
+      reinterpret_cast<ulonglong2*>(tables), n2);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_topk(const QueryView& qv, uint32_t q_begin, uint32_t q_count, uint32_t k, uint32_t* out_ids,

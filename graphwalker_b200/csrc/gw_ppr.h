@@ -9,6 +9,13 @@ constexpr int kPprThreads = 256;
 constexpr int kTopkThreads = 512;
 constexpr uint32_t kTopkBuffer = 1024;  // candidate keys per CTA
 constexpr uint32_t kTopkMaxK = kTopkBuffer - kTopkThreads;
+constexpr uint32_t kTopkUnroll = 8;     // table slots a top-k thread loads at once
+
+// Walks a warp takes from the batch cursor at a time: small enough that the
+// walks in flight stay inside a narrow window of the batch (and of its
+// queries), large enough that the cursor's atomic is not contended (64 and
+// 1024 were both slower at R-MAT scale 26 with 4096 queries).
+constexpr uint32_t kWarpChunk = 256;
 
 struct QueryView {
   const uint32_t* sources;                 // nq source vertices
@@ -20,6 +27,7 @@ struct QueryView {
   uint32_t* full;                          // nq: set to 1 when query q's table filled up
   const uint32_t* stream;                  // nq: Philox stream word of query q (NULL = 0)
   unsigned long long* visits;              // total visits counter (may be NULL)
+  unsigned long long* cursor;              // batch positions handed out (zeroed by the launcher)
   uint32_t nq;
 };
 
@@ -27,6 +35,8 @@ struct QueryView {
 cudaError_t launch_walk_queries(int rule, const QueryView& qv, unsigned long long w_begin,
                                 unsigned long long w_end, const GraphView& g, const WalkArgs& a,
                                 uint32_t* status, int threads_per_sm, cudaStream_t stream);
+// Sets slots [0, n) of a table area to empty.
+cudaError_t launch_clear_tables(unsigned long long* tables, unsigned long long n, cudaStream_t stream);
 // Top-k of queries [q_begin, q_begin + q_count) into out[q * k + r].
 cudaError_t launch_topk(const QueryView& qv, uint32_t q_begin, uint32_t q_count, uint32_t k, uint32_t* out_ids,
                         uint32_t* out_counts, cudaStream_t stream);

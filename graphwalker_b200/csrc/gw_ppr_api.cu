@@ -29,15 +29,16 @@ struct QuerySet {
   std::vector<unsigned long long> prefix, id_base, toff;
   std::vector<uint32_t> tmask;
   uint64_t walks = 0, slots = 0;
-  gw_devbuf own[9];
-  gw_devbuf *d_sources, *d_prefix, *d_id_base, *d_toff, *d_tmask, *d_tables, *d_full, *d_ids, *d_cnt;
+  gw_devbuf own[10];
+  gw_devbuf *d_sources, *d_prefix, *d_id_base, *d_toff, *d_tmask, *d_tables, *d_full, *d_ids, *d_cnt, *d_cursor;
   gw::QueryView qv{};
 
   QuerySet(gw_ctx* ctx, bool use_ctx_buffers) {
-    gw_devbuf* b[9] = {&ctx->d_q_sources, &ctx->d_q_prefix, &ctx->d_q_idbase, &ctx->d_q_toff, &ctx->d_q_tmask,
-                       &ctx->d_q_tables, &ctx->d_q_full, &ctx->d_q_ids, &ctx->d_q_counts};
-    gw_devbuf** d[9] = {&d_sources, &d_prefix, &d_id_base, &d_toff, &d_tmask, &d_tables, &d_full, &d_ids, &d_cnt};
-    for (int i = 0; i < 9; ++i) *d[i] = use_ctx_buffers ? b[i] : &own[i];
+    gw_devbuf* b[10] = {&ctx->d_q_sources, &ctx->d_q_prefix, &ctx->d_q_idbase, &ctx->d_q_toff, &ctx->d_q_tmask,
+                        &ctx->d_q_tables, &ctx->d_q_full, &ctx->d_q_ids, &ctx->d_q_counts, &ctx->d_q_cursor};
+    gw_devbuf** d[10] = {&d_sources, &d_prefix, &d_id_base, &d_toff, &d_tmask,
+                         &d_tables, &d_full, &d_ids, &d_cnt, &d_cursor};
+    for (int i = 0; i < 10; ++i) *d[i] = use_ctx_buffers ? b[i] : &own[i];
   }
   ~QuerySet() {
     for (auto& b : own) b.release();
@@ -81,6 +82,7 @@ gw_status upload_set(gw_ctx* ctx, QuerySet* s, uint32_t k, cudaStream_t st) {
   GW_CUDA(ctx, s->d_full->ensure(n * 4), "query alloc");
   GW_CUDA(ctx, s->d_ids->ensure((uint64_t)n * k * 4), "top-k alloc");
   GW_CUDA(ctx, s->d_cnt->ensure((uint64_t)n * k * 4), "top-k alloc");
+  GW_CUDA(ctx, s->d_cursor->ensure(sizeof(unsigned long long)), "query alloc");
   GW_CUDA(ctx, cudaMemcpyAsync(s->d_sources->p, s->sources.data(), n * 4, cudaMemcpyHostToDevice, st), "copy");
   GW_CUDA(ctx, cudaMemcpyAsync(s->d_prefix->p, s->prefix.data(), (n + 1) * 8, cudaMemcpyHostToDevice, st), "copy");
   GW_CUDA(ctx, cudaMemcpyAsync(s->d_id_base->p, s->id_base.data(), n * 8, cudaMemcpyHostToDevice, st), "copy");
@@ -94,6 +96,7 @@ gw_status upload_set(gw_ctx* ctx, QuerySet* s, uint32_t k, cudaStream_t st) {
   s->qv.table_mask = s->d_tmask->as<uint32_t>();
   s->qv.tables = s->d_tables->as<unsigned long long>();
   s->qv.full = s->d_full->as<uint32_t>();
+  s->qv.cursor = s->d_cursor->as<unsigned long long>();
   s->qv.nq = n;
   return GW_OK;
 }
@@ -112,7 +115,7 @@ cudaError_t run_set(gw_ctx* ctx, const gw_walk_params* p, const gw::WalkArgs& a,
   const uint32_t n = s->qv.nq;
   cudaEventRecord(ev[0], st);
   if (batched) {
-    e = cudaMemsetAsync(s->qv.tables, 0xff, s->slots * 8, st);
+    e = gw::launch_clear_tables(s->qv.tables, s->slots, st);
     cudaEventRecord(ev[1], st);
     if (e == cudaSuccess)
       e = gw::launch_walk_queries((int)p->rule, s->qv, 0, s->walks, ctx->view(), a, ctx->d_status.as<uint32_t>(),
@@ -124,7 +127,7 @@ cudaError_t run_set(gw_ctx* ctx, const gw_walk_params* p, const gw::WalkArgs& a,
   } else {
     cudaEventRecord(ev[1], st);
     for (uint32_t q = 0; q < n && e == cudaSuccess; ++q) {
-      e = cudaMemsetAsync(s->qv.tables + s->toff[q], 0xff, ((uint64_t)s->tmask[q] + 1) * 8, st);
+      e = gw::launch_clear_tables(s->qv.tables + s->toff[q], (uint64_t)s->tmask[q] + 1, st);
       if (e == cudaSuccess)
         e = gw::launch_walk_queries((int)p->rule, s->qv, s->prefix[q], s->prefix[q + 1], ctx->view(), a,
                                     ctx->d_status.as<uint32_t>(), 0, st);
@@ -248,7 +251,7 @@ extern "C" gw_status gw_ppr_autotune(gw_ctx* ctx, const gw_walk_params* params, 
   for (int c : candidates) {
     float ms_sum = 0.f;
     for (int rep = 0; rep < 3; ++rep) {
-      cudaMemsetAsync(set.qv.tables, 0xff, set.slots * 8, st);
+      gw::launch_clear_tables(set.qv.tables, set.slots, st);
       cudaEventRecord(e0, st);
       gw::launch_walk_queries((int)params->rule, set.qv, 0, set.walks, ctx->view(), a, ctx->d_status.as<uint32_t>(),
                               c, st);

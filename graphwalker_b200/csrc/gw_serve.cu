@@ -120,19 +120,22 @@ struct gw_server {
 
 namespace {
 
-// Staging layout for up to n queries in one superstep (8-byte fields first).
+// Staging layout for up to n queries in one superstep: the launch's chunk
+// cursor, then the 8-byte and 4-byte per-query fields, then the top-k output.
 struct Stage {
-  unsigned long long *prefix, *id_base, *toff;
+  unsigned long long *cursor, *prefix, *id_base, *toff;
   uint32_t *sources, *tmask, *full, *stream, *ids, *counts;
 };
 
 size_t stage_bytes(uint32_t n, uint32_t k) {
-  return (size_t)(n + 1) * 8 + 2 * (size_t)n * 8 + 4 * (size_t)n * 4 + 2 * (size_t)n * k * 4;
+  return 8 + (size_t)(n + 1) * 8 + 2 * (size_t)n * 8 + 4 * (size_t)n * 4 + 2 * (size_t)n * k * 4;
 }
 
 Stage carve(void* base, uint32_t n, uint32_t k) {
   Stage s;
   char* p = static_cast<char*>(base);
+  s.cursor = reinterpret_cast<unsigned long long*>(p);
+  p += 8;
   s.prefix = reinterpret_cast<unsigned long long*>(p);
   p += (size_t)(n + 1) * 8;
   s.id_base = reinterpret_cast<unsigned long long*>(p);
@@ -163,6 +166,7 @@ gw::QueryView make_view(const Stage& d, unsigned long long* tables, uint32_t n) 
   qv.tables = tables;
   qv.full = d.full;
   qv.stream = d.stream;
+  qv.cursor = d.cursor;
   qv.nq = n;
   return qv;
 }
@@ -222,7 +226,7 @@ bool superstep(gw_server* srv) {
     for (uint64_t tk : chosen) cq.push_back(&srv->queries[tk]);
   }
   for (Query* q : admitted)
-    cudaMemsetAsync(srv->tables.as<unsigned long long>() + q->table_off, 0xff, q->table_slots * 8, st);
+    gw::launch_clear_tables(srv->tables.as<unsigned long long>() + q->table_off, q->table_slots, st);
   if (chosen.empty()) return true;
   const uint32_t n = (uint32_t)chosen.size();
   if (n > srv->stage_cap) {
@@ -249,7 +253,7 @@ bool superstep(gw_server* srv) {
     acc += take[i];
   }
   h.prefix[n] = acc;
-  const size_t head = stage_bytes(n, k) - 2 * (size_t)n * k * 4;
+  const size_t head = stage_bytes(n, k) - 8 - 2 * (size_t)n * k * 4;
   cudaError_t e = cudaMemcpyAsync(d.prefix, h.prefix, head, cudaMemcpyHostToDevice, st);
   gw::QueryView qv = make_view(d, srv->tables.as<unsigned long long>(), n);
   if (e == cudaSuccess)
@@ -291,7 +295,7 @@ bool superstep(gw_server* srv) {
         q.table_off = off;
         q.table_slots = slots;
         srv->active.push_back(chosen[i]);
-        cudaMemsetAsync(srv->tables.as<unsigned long long>() + off, 0xff, slots * 8, st);
+        gw::launch_clear_tables(srv->tables.as<unsigned long long>() + off, slots, st);
       } else {
         srv->pending.push_front(chosen[i]);  // waits at the head of the queue for space
       }
