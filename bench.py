@@ -41,7 +41,13 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "walk-steps/s"
 FALLBACK_HBM_GBS = 6650.0
-BYTES_PER_STEP = 64  # one 32-B sector for the vertex record + one for the column id
+# Algorithmic DRAM bytes of the headline kernel, per graph layout:
+#   csr:  per step one 32-B sector for the vertex record + one for the column id;
+#   erec: per step one 32-B sector (the edge record moved along, or the vertex
+#         record of a jump target) + one 32-B sector per walk for its start record.
+BYTES_PER_STEP = {"csr": 64, "erec": 32}
+BYTES_PER_WALK = {"csr": 0, "erec": 32}
+LAYOUT_MODE = {"auto": 2, "csr": 0, "erec": 1}  # EDGE_RECORDS_AUTO / _OFF / _ON
 
 
 def parse_args():
@@ -57,6 +63,8 @@ def parse_args():
     ap.add_argument("--graph-seed", type=int, default=1)
     ap.add_argument("--walk-seed", type=int, default=42)
     ap.add_argument("--aggregate", type=int, default=0, help="warp-aggregated counter atomics")
+    ap.add_argument("--layout", choices=["auto", "csr", "erec"], default="auto",
+                    help="graph layout of resident walks: edge records when they fit (auto), plain CSR, edge records")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-probe", action="store_true", help="skip the random-gather roof probe")
@@ -161,9 +169,9 @@ def measured_peaks() -> tuple[float, str]:
     return FALLBACK_HBM_GBS, "fallback"
 
 
-def profile_traffic() -> float | None:
+def profile_traffic(layout: str) -> float | None:
     """DRAM bytes per walk launch from the committed ncu summary, if any."""
-    f = ROOT / "profiles" / "walk_resident_rmat24.json"
+    f = ROOT / "profiles" / ("walk_resident_rmat24.json" if layout == "csr" else "walk_resident_erec_rmat24.json")
     if f.exists():
         try:
             return float(json.loads(f.read_text())["dram_bytes_per_launch"])
@@ -310,6 +318,7 @@ def our_arm(args) -> None:
 
     kb = blocksize_kb_for(args.scale, args.edge_factor, args.nblocks)
     G = gw.Graph.rmat(args.scale, args.edge_factor, seed=args.graph_seed, blocksize_kb=kb, device=local)
+    layout = "erec" if G.set_edge_records(LAYOUT_MODE[args.layout]) else "csr"
     nv, L = G.nv, args.L
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
@@ -423,18 +432,22 @@ def our_arm(args) -> None:
         G.close()
         return
     peak, peak_kind = measured_peaks()
-    achieved = BYTES_PER_STEP * steps_per_launch / (kern_ms * 1e-3) / 1e9
-    traffic = profile_traffic()
+    algo_bytes = BYTES_PER_STEP[layout] * steps_per_launch + BYTES_PER_WALK[layout] * nv
+    achieved = algo_bytes / (kern_ms * 1e-3) / 1e9
+    traffic = profile_traffic(layout)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "peak_source": f"{peak_kind} HBM copy bandwidth",
-            "bytes_per_step": BYTES_PER_STEP, "kernel": "walk_resident_kernel<JUMP, VERTEX_COUNT>",
+            "bytes_per_step": BYTES_PER_STEP[layout], "bytes_per_walk": BYTES_PER_WALK[layout],
+            "algorithmic_bytes_per_launch": algo_bytes, "graph_layout": layout,
+            "kernel": f"walk_resident_kernel<JUMP, VERTEX_COUNT, ER={'true' if layout == 'erec' else 'false'}>",
             "kernel_ms": kern_ms}
     if gather_bps:
         roof["gather_peak_gbs"] = gather_bps / 1e9
         roof["gather_frac"] = achieved / (gather_bps / 1e9)
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
             "warmup": max(3, args.warmup), "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": workload_config(args, G.nblocks),
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {**workload_config(args, G.nblocks), "graph_layout": layout},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": K, "clocks": clk.summary(),
             "walk_steps_per_step": steps_per_launch * world}
     G.close()
@@ -463,6 +476,7 @@ def msppr_arm(args) -> None:
     scale = args.scale if args.scale != 24 else 26
     kb = blocksize_kb_for(scale, args.edge_factor, args.nblocks)
     G = gw.Graph.rmat(scale, args.edge_factor, seed=args.graph_seed, blocksize_kb=kb)
+    layout = "erec" if G.set_edge_records(LAYOUT_MODE[args.layout]) else "csr"
     rp, _ = G.export_csr()
     sources, budgets = msppr_queries(rp, args.queries)
     del rp
@@ -506,7 +520,8 @@ def msppr_arm(args) -> None:
             "config": {"workload": f"multi-source PPR, R-MAT scale {scale} ef {args.edge_factor}, {args.queries} queries, "
                                    f"sources uniform over out-degree>=1, budgets round(10^U(2,5)), stop rule p=0.15, "
                                    f"L<=20, top-{args.topk}",
-                       "walks_per_step": int(budgets.sum()), "autotuned_threads_per_sm": tuned},
+                       "walks_per_step": int(budgets.sum()), "autotuned_threads_per_sm": tuned,
+                       "graph_layout": layout},
             "breakdown_ms": {"clear": statistics.median(r[1] for r in runs),
                              "walk": statistics.median(r[2] for r in runs),
                              "topk": statistics.median(r[3] for r in runs)},

@@ -37,6 +37,7 @@ class WalkParams(Structure):
 
 
 SERVE_BATCHED, SERVE_PLAIN = 0, 1
+EDGE_RECORDS_OFF, EDGE_RECORDS_ON, EDGE_RECORDS_AUTO = 0, 1, 2
 
 
 class ServeConfig(Structure):
@@ -131,6 +132,7 @@ _SIGS = {
     "gw_serve_close": (c_int32, [_P]),
     "gw_set_l2_fetch_granularity": (c_int32, [_P, c_uint32, POINTER(c_uint32)]),
     "gw_set_l2_persisting": (c_int32, [_P, c_uint64]),
+    "gw_set_edge_records": (c_int32, [_P, c_uint32, POINTER(c_uint32)]),
 }
 
 _lib = None

@@ -65,6 +65,36 @@ gw_status init_ctx(gw_ctx* ctx, int device) {
   GW_CUDA(ctx, ctx->d_status.ensure(sizeof(uint32_t)), "status alloc");
   GW_CUDA(ctx, ctx->h_status.ensure(sizeof(uint32_t)), "status alloc");
   GW_CUDA(ctx, cudaMemsetAsync(ctx->d_status.p, 0, sizeof(uint32_t), ctx->stream), "memset");
+  const char* env = getenv("GW_EDGE_RECORDS");
+  ctx->erec_mode = env && strcmp(env, "0") == 0 ? GW_EDGE_RECORDS_OFF : GW_EDGE_RECORDS_AUTO;
+  return GW_OK;
+}
+
+// Builds or drops the edge records of a graph as ctx->erec_mode and the
+// residency say (see gw_set_edge_records).
+gw_status apply_edge_records(gw_ctx* ctx) {
+  if (ctx->residency != GW_RESIDENT_HBM || ctx->erec_mode == GW_EDGE_RECORDS_OFF) {
+    ctx->d_erec.release();
+    return GW_OK;
+  }
+  const size_t bytes = (size_t)ctx->ne * sizeof(ulonglong2);
+  if (ctx->d_erec.p && ctx->d_erec.bytes >= bytes) return GW_OK;
+  GW_CUDA(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (ctx->erec_mode == GW_EDGE_RECORDS_AUTO) {
+    size_t free_b = 0, total_b = 0;
+    GW_CUDA(ctx, cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    if (bytes > free_b / 2) return GW_OK;
+  }
+  if (ctx->d_erec.ensure(bytes) != cudaSuccess) {
+    cudaGetLastError();  // an allocation failure is not sticky
+    ctx->d_erec.release();
+    if (ctx->erec_mode == GW_EDGE_RECORDS_ON)
+      return ctx->fail(GW_E_NOMEM, "edge records: %zu bytes do not fit on the device", bytes);
+    return GW_OK;
+  }
+  GW_CUDA(ctx, gw::launch_build_erec(ctx->d_colidx.as<uint32_t>(), ctx->d_vrec.as<unsigned long long>(), ctx->ne,
+                                     ctx->nv, ctx->d_erec.as<ulonglong2>(), ctx->stream), "build_erec");
+  GW_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "build_erec");
   return GW_OK;
 }
 
@@ -298,6 +328,7 @@ gw_status gw_open(const gw_graph_desc* desc, gw_ctx** out) {
     ctx->h_rowptr.release();
     ctx->h_colidx.release();
   }
+  if (s == GW_OK) s = apply_edge_records(ctx);
   if (s != GW_OK) {
     set_thread_error(s, ctx->err);
     gw_close(ctx);
@@ -320,6 +351,7 @@ gw_status gw_open_csr(const uint64_t* rowptr, const uint32_t* colidx, uint32_t n
   static const uint32_t kNoEdges = 0;
   if (s == GW_OK)
     s = install_graph(ctx, rowptr, colidx ? colidx : &kNoEdges, nvertices, blocks, nblocks);
+  if (s == GW_OK) s = apply_edge_records(ctx);
   if (s != GW_OK) {
     set_thread_error(s, ctx->err);
     gw_close(ctx);
@@ -378,6 +410,7 @@ gw_status gw_open_rmat(uint32_t scale, uint32_t edge_factor, uint64_t seed, doub
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) s = ctx->cuda_fail(e, "rmat install");
   }
+  if (s == GW_OK) s = apply_edge_records(ctx);
   if (s != GW_OK) {
     set_thread_error(s, ctx->err);
     gw_close(ctx);
@@ -393,7 +426,7 @@ gw_status gw_close(gw_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   if (ctx->l2_persist_bytes) gw_set_l2_persisting(ctx, 0);
-  for (gw_devbuf* b : {&ctx->d_rowptr, &ctx->d_colidx, &ctx->d_vrec, &ctx->d_blocks, &ctx->d_status,
+  for (gw_devbuf* b : {&ctx->d_rowptr, &ctx->d_colidx, &ctx->d_vrec, &ctx->d_erec, &ctx->d_blocks, &ctx->d_status,
                        &ctx->d_walks, &ctx->d_words, &ctx->d_ids, &ctx->d_counts, &ctx->d_paths,
                        &ctx->d_plen, &ctx->d_closure, &ctx->d_pool_offsets, &ctx->d_dest,
                        &ctx->d_tile_hist, &ctx->d_tile_off, &ctx->d_totals, &ctx->d_minhop,
@@ -458,6 +491,7 @@ gw_status gw_set_residency(gw_ctx* ctx, uint32_t residency, uint32_t nmblocks) {
     ctx->d_rowptr.release();
     ctx->d_colidx.release();
     ctx->d_vrec.release();
+    ctx->d_erec.release();
   } else {
     GW_CUDA(ctx, ctx->d_rowptr.ensure(rp), "rowptr alloc");
     GW_CUDA(ctx, ctx->d_colidx.ensure(ci), "colidx alloc");
@@ -471,7 +505,17 @@ gw_status gw_set_residency(gw_ctx* ctx, uint32_t residency, uint32_t nmblocks) {
     ctx->h_colidx.release();
   }
   ctx->residency = residency;
-  return GW_OK;
+  return apply_edge_records(ctx);
+}
+
+gw_status gw_set_edge_records(gw_ctx* ctx, uint32_t mode, uint32_t* built) {
+  if (!ctx) return set_thread_error(GW_E_INVALID, "NULL context");
+  if (mode > GW_EDGE_RECORDS_AUTO) return ctx->fail(GW_E_INVALID, "unknown edge-record mode %u", mode);
+  ctx->erec_mode = mode;
+  if (mode == GW_EDGE_RECORDS_OFF) ctx->d_erec.release();
+  const gw_status s = apply_edge_records(ctx);
+  if (built) *built = ctx->view().erec ? 1u : 0u;
+  return s;
 }
 
 gw_status gw_walks_clear(gw_ctx* ctx) {

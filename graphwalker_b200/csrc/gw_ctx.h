@@ -69,6 +69,8 @@ struct gw_ctx {
   uint32_t nblocks = 0;
   std::vector<uint32_t> blocks;  // nblocks + 1
   gw_devbuf d_rowptr, d_colidx, d_vrec, d_blocks;
+  gw_devbuf d_erec;                     // edge records (empty = not built)
+  uint32_t erec_mode = GW_EDGE_RECORDS_AUTO;
   gw_hostbuf h_rowptr, h_colidx;  // pinned copy (streaming residency)
 
   // device status word (+ pinned mirror)
@@ -138,6 +140,7 @@ struct gw_ctx {
     g.vrec = d_vrec.as<const unsigned long long>();
     g.rowptr = d_rowptr.as<const unsigned long long>();
     g.colidx = d_colidx.as<const uint32_t>();
+    g.erec = d_erec.p && d_erec.bytes >= ne * sizeof(ulonglong2) ? d_erec.as<const ulonglong2>() : nullptr;
     g.nv = nv;
     return g;
   }

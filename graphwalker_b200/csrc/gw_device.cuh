@@ -79,6 +79,14 @@ __device__ __forceinline__ unsigned long long ld_nc_u64(const unsigned long long
   return r;
 }
 
+__device__ __forceinline__ ulonglong2 ld_nc_u64x2(const ulonglong2* a, uint64_t pol) {
+  ulonglong2 r;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u64 {%0, %1}, [%2], %3;"
+               : "=l"(r.x), "=l"(r.y)
+               : "l"(a), "l"(pol));
+  return r;
+}
+
 __device__ __forceinline__ void red_add_u32(uint32_t* a, uint32_t v, uint64_t pol) {
   asm volatile("red.relaxed.gpu.global.add.L2::cache_hint.u32 [%0], %1, %2;" ::"l"(a), "r"(v), "l"(pol)
                : "memory");
@@ -101,6 +109,10 @@ struct GraphView {
   const unsigned long long* __restrict__ vrec;    // packed vertex records (nv)
   const unsigned long long* __restrict__ rowptr;  // row pointer (nv + 1)
   const uint32_t* __restrict__ colidx;
+  // Edge records (one per edge, NULL when not built): x = the packed record
+  // of the edge's target, y = the target's id.  Moving along an edge then
+  // reads the next vertex and its record in one 16-byte load.
+  const ulonglong2* __restrict__ erec;
   uint32_t nv;
 };
 
@@ -182,6 +194,65 @@ __device__ __forceinline__ bool hop_advance_rec(const GraphView& g, const WalkAr
     return false;
   }
   return false;  // STOP, PROB
+}
+
+// v's packed record, or 0 (no edges) when v is out of range: the caller's
+// bounds check ends the walk before that record is used.
+__device__ __forceinline__ unsigned long long vertex_rec(const GraphView& g, const L2Hints& hp, uint32_t v) {
+  return v < g.nv ? ld_nc_u64(g.vrec + v, hp.rec) : 0ull;
+}
+
+// The same hop over the edge-record layout: the record of v is carried in
+// `rec` from the previous hop.  Moving along an edge reads the next vertex and
+// its record together; a jump reads the record of its target; a return to the
+// source takes the source's record, src_rec, held by the caller.
+template <int RULE>
+__device__ __forceinline__ bool hop_advance_carried(const GraphView& g, const WalkArgs& a, const L2Hints& hp,
+                                                    uint32_t id, uint32_t src, unsigned long long src_rec,
+                                                    uint32_t hop, uint32_t& v, unsigned long long& rec,
+                                                    uint32_t stream = 0u) {
+  const Philox4 ph = philox4x32_10(id, hop, stream, 0u, a.seed_lo, a.seed_hi);
+  const uint32_t d0 = ph.x >> 1;
+  const uint32_t d1 = ph.y >> 1;
+  unsigned long long off = rec >> kDegBits;
+  unsigned long long deg = rec & kDegEscape;
+  if (deg == kDegEscape) {  // mega-hub: exact degree from the row pointer
+    const unsigned long long b = __ldg(g.rowptr + v);
+    deg = __ldg(g.rowptr + v + 1) - b;
+    off = b;
+  }
+  if (deg > 0 && d0 >= a.thr) {
+    const unsigned long long r =
+        deg > 0x7fffffffull ? (unsigned long long)d1 : (unsigned long long)(d1 % (uint32_t)deg);
+    const ulonglong2 e = ld_nc_u64x2(g.erec + off + r, hp.col);
+    v = (uint32_t)e.y;
+    rec = e.x;
+    return true;
+  }
+  const uint32_t dj = deg > 0 ? d1 : d0;
+  if (RULE == GW_RULE_JUMP) {
+    v = dj % a.njump;
+    rec = vertex_rec(g, hp, v);
+    return true;
+  } else if (RULE == GW_RULE_RESTART) {
+    v = src;
+    rec = src_rec;
+    return true;
+  } else if (RULE == GW_RULE_PPR) {
+    if (deg == 0) {
+      v = src;
+      rec = src_rec;
+      return true;
+    }
+    return false;
+  }
+  return false;  // STOP, PROB
+}
+
+// Whether a rule's hop can return a walk to its source.
+template <int RULE>
+__device__ __forceinline__ constexpr bool rule_returns() {
+  return RULE == GW_RULE_RESTART || RULE == GW_RULE_PPR;
 }
 
 // Same hop over a block-local CSR slice (streamed blocks): beg_pos is the

@@ -102,7 +102,7 @@ __device__ __forceinline__ uint32_t query_of(const unsigned long long* __restric
   return lo;
 }
 
-template <int RULE>
+template <int RULE, bool ER>
 __global__ void __launch_bounds__(kPprThreads)
     walk_query_kernel(QueryView qv, unsigned long long w_begin, unsigned long long w_end, GraphView g,
                       WalkArgs a, uint32_t* __restrict__ status) {
@@ -118,6 +118,7 @@ __global__ void __launch_bounds__(kPprThreads)
   bool drained = false;                      // the cursor has run past the batch (warp-uniform)
   bool busy = false;                         // this lane holds a walk
   unsigned long long j = 0, id_shift = 0, q_lo = 1, q_hi = 0;
+  unsigned long long cur_rec = 0, src_rec = 0;  // edge-record mode: records of v and of the source
   uint32_t q = 0, src = 0, sid = 0, v = 0, hop = 0, st = 0, nvisit = 0;
   for (;;) {
     // Idle lanes take the next walks of the warp's chunk, in lane order.
@@ -146,6 +147,7 @@ __global__ void __launch_bounds__(kPprThreads)
           // stream id = the walk's position in the original batch
           id_shift = qv.id_base ? __ldg(qv.id_base + q) - q_lo : 0ull;
           sid = qv.stream ? __ldg(qv.stream + q) : 0u;
+          if (ER) src_rec = vertex_rec(g, hp, src);
         }
         const unsigned long long lo = q_lo > w_begin ? q_lo : w_begin, hi = q_hi < w_end ? q_hi : w_end;
         if (visits_source && j == lo && src < g.nv &&
@@ -153,6 +155,7 @@ __global__ void __launch_bounds__(kPprThreads)
                        hp.cnt))
           qv.full[q] = 1u;
         v = src;
+        cur_rec = src_rec;
         hop = 0;
       }
       const uint32_t n_idle = __popc(idle);
@@ -171,7 +174,7 @@ __global__ void __launch_bounds__(kPprThreads)
       st |= kStBounds;
       end = true;
     } else {
-      const unsigned long long rec = ld_nc_u64(g.vrec + v, hp.rec);
+      const unsigned long long rec = ER ? cur_rec : ld_nc_u64(g.vrec + v, hp.rec);
       ++nvisit;
       // Table update for hops >= 1: lanes visiting the same (query, vertex)
       // fold into one; its first probe (a CAS) is issued now and resolved
@@ -201,22 +204,35 @@ __global__ void __launch_bounds__(kPprThreads)
         deg = __ldg(g.rowptr + v + 1) - off;
       }
       uint32_t next = v;
+      unsigned long long next_rec = 0;
       bool moved = true;
       if (deg > 0 && d0 >= a.thr) {
         const unsigned long long r =
             deg > 0x7fffffffull ? (unsigned long long)d1 : (unsigned long long)(d1 % (uint32_t)deg);
-        next = ld_nc_u32(g.colidx + off + r, hp.col);
+        if (ER) {
+          const ulonglong2 e = ld_nc_u64x2(g.erec + off + r, hp.col);
+          next = (uint32_t)e.y;
+          next_rec = e.x;
+        } else {
+          next = ld_nc_u32(g.colidx + off + r, hp.col);
+        }
       } else {
         const uint32_t dj = deg > 0 ? d1 : d0;
-        if (RULE == GW_RULE_JUMP) next = dj % a.njump;
-        else if (RULE == GW_RULE_RESTART) next = src;
-        else if (RULE == GW_RULE_PPR && deg == 0) next = src;
-        else moved = false;
+        if (RULE == GW_RULE_JUMP) {
+          next = dj % a.njump;
+          if (ER) next_rec = vertex_rec(g, hp, next);
+        } else if (RULE == GW_RULE_RESTART || (RULE == GW_RULE_PPR && deg == 0)) {
+          next = src;
+          next_rec = src_rec;
+        } else {
+          moved = false;
+        }
       }
       if (leader && !table_finish(t, mask, s0, old, v, n, hp.cnt)) qv.full[q] = 1u;
       end = !moved;
       if (moved) {
         v = next;
+        cur_rec = next_rec;
         ++hop;
         if (RULE == GW_RULE_RESTART && hop % a.L == a.L - 1) end = true;
       }
@@ -324,7 +340,7 @@ template <int RULE>
 cudaError_t query_dispatch(const QueryView& qv, unsigned long long w_begin, unsigned long long w_end,
                            const GraphView& g, const WalkArgs& a, uint32_t* status, int threads_per_sm,
                            cudaStream_t stream) {
-  auto kern = walk_query_kernel<RULE>;
+  auto kern = g.erec ? walk_query_kernel<RULE, true> : walk_query_kernel<RULE, false>;
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPprThreads, 0);
   const int sms = sm_count();

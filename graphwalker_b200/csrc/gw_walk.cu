@@ -9,6 +9,8 @@
 // iteration, so lanes never wait for the longest walk of their warp.  Per hop:
 // one 8-byte packed vertex record load, one 4-byte column load, one Philox
 // block computed while the record load is in flight, and one visit atomic.
+// With edge records (ER) the record of the current vertex is carried from the
+// previous hop, so a hop along an edge is a single 16-byte gather.
 #include "gw_internal.h"
 
 namespace gw {
@@ -19,7 +21,7 @@ __device__ __forceinline__ uint4 load_walk(const gw_walk_rec* __restrict__ walks
   return __ldg(reinterpret_cast<const uint4*>(walks) + i);
 }
 
-template <int RULE, int SINK, bool AGG>
+template <int RULE, int SINK, bool AGG, bool ER>
 __global__ void __launch_bounds__(kWalkThreads)
     walk_resident_kernel(const gw_walk_rec* __restrict__ walks, uint64_t n, GraphView g,
                          WalkArgs a, SinkView s, uint32_t* __restrict__ status) {
@@ -31,6 +33,12 @@ __global__ void __launch_bounds__(kWalkThreads)
   uint32_t st = 0;
   uint32_t clos = 0;
   const L2Hints hp = make_hints(a.hints);
+  // edge-record mode: the records of the current vertex and of the source
+  unsigned long long rec = 0, src_rec = 0;
+  if (ER) {
+    rec = vertex_rec(g, hp, v);
+    if (rule_returns<RULE>()) src_rec = src == v ? rec : vertex_rec(g, hp, src);
+  }
   for (;;) {
     bool end;
     if (rule_capped<RULE>() && hop >= a.L) {
@@ -52,7 +60,8 @@ __global__ void __launch_bounds__(kWalkThreads)
         clos += ((int)hop >= (int)a.L - 1 && v == src) ? 1u : 0u;
       }
       ++k;
-      end = !hop_advance<RULE>(g, a, hp, id, src, hop, v);
+      end = ER ? !hop_advance_carried<RULE>(g, a, hp, id, src, src_rec, hop, v, rec)
+               : !hop_advance<RULE>(g, a, hp, id, src, hop, v);
       if (!end) {
         ++hop;
         if (RULE == GW_RULE_RESTART && hop % a.L == a.L - 1) end = true;
@@ -68,10 +77,24 @@ __global__ void __launch_bounds__(kWalkThreads)
       src = w.z;
       hop = w.w;
       k = 0;
+      if (ER) {
+        rec = vertex_rec(g, hp, v);
+        if (rule_returns<RULE>()) src_rec = src == v ? rec : vertex_rec(g, hp, src);
+      }
     }
   }
   if (st) atomicOr(status, st);
   if (SINK == GW_SINK_CLOSURE_COUNT && clos) atomicAdd(s.closure, (unsigned long long)clos);
+}
+
+// Edge records: erec[e] = (packed record of colidx[e], colidx[e]).
+__global__ void build_erec_kernel(const uint32_t* __restrict__ colidx, const unsigned long long* __restrict__ vrec,
+                                  uint64_t ne, uint32_t nv, ulonglong2* __restrict__ erec) {
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < ne;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t w = __ldg(colidx + e);
+    erec[e] = make_ulonglong2(w < nv ? __ldg(vrec + w) : 0ull, (unsigned long long)w);
+  }
 }
 
 __device__ __forceinline__ uint32_t find_block(const uint32_t* __restrict__ blocks,
@@ -258,7 +281,7 @@ template <int RULE, int SINK, bool AGG>
 cudaError_t resident_dispatch(const gw_walk_rec* walks, uint64_t n, const GraphView& g,
                               const WalkArgs& a, const SinkView& s, uint32_t* status, int grid,
                               cudaStream_t stream, const cudaAccessPolicyWindow* window) {
-  auto k = walk_resident_kernel<RULE, SINK, AGG>;
+  auto k = g.erec ? walk_resident_kernel<RULE, SINK, AGG, true> : walk_resident_kernel<RULE, SINK, AGG, false>;
   if (grid <= 0) grid = occupancy_grid(k, n);
   if (!window) {
     k<<<grid, kWalkThreads, 0, stream>>>(walks, n, g, a, s, status);
@@ -278,7 +301,10 @@ cudaError_t resident_dispatch(const gw_walk_rec* walks, uint64_t n, const GraphV
 
 template <int RULE, int SINK, bool AGG>
 int resident_grid(uint64_t n) {
-  return occupancy_grid(walk_resident_kernel<RULE, SINK, AGG>, n);
+  // both variants have the same block shape; the larger register count bounds the grid
+  const int a = occupancy_grid(walk_resident_kernel<RULE, SINK, AGG, false>, n);
+  const int b = occupancy_grid(walk_resident_kernel<RULE, SINK, AGG, true>, n);
+  return a < b ? a : b;
 }
 
 template <int RULE, int SINK, bool AGG>
@@ -374,6 +400,13 @@ cudaError_t launch_pack_words(const gw_walk_rec* walks, uint64_t n, const uint32
   if (n == 0) return cudaSuccess;
   pack_words_kernel<<<elementwise_grid(n), 256, 0, stream>>>(walks, n, blocks, nblocks, words,
                                                              wblock);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_build_erec(const uint32_t* colidx, const unsigned long long* vrec, uint64_t ne, uint32_t nv,
+                              ulonglong2* erec, cudaStream_t stream) {
+  if (ne == 0) return cudaSuccess;
+  build_erec_kernel<<<elementwise_grid(ne), 256, 0, stream>>>(colidx, vrec, ne, nv, erec);
   return cudaGetLastError();
 }
 

@@ -273,6 +273,12 @@ class Graph:
     def set_l2_persisting(self, nbytes: int) -> None:
         check(load().gw_set_l2_persisting(self._h, nbytes), self._h)
 
+    def set_edge_records(self, mode: int) -> bool:
+        """EDGE_RECORDS_OFF / _ON / _AUTO (gw_set_edge_records); True when in use."""
+        built = c_uint32()
+        check(load().gw_set_edge_records(self._h, mode, byref(built)), self._h)
+        return bool(built.value)
+
     def probe_gather(self, buf, n_words: int, loads: int, iters: int = 5) -> float:
         out = c_double()
         check(load().gw_probe_gather(self._h, _ptr(buf), n_words, loads, iters, byref(out)), self._h)

@@ -325,6 +325,24 @@ gw_status gw_set_l2_fetch_granularity(gw_ctx *ctx, uint32_t bytes, uint32_t *pre
    policy window on the launch).  0 releases the reservation.               */
 gw_status gw_set_l2_persisting(gw_ctx *ctx, uint64_t bytes);
 
+/* ---- graph layout -------------------------------------------------------- */
+/* Edge records: a second copy of the column array in which each edge also
+   carries its target's packed (first-edge offset, out-degree) record, 16 bytes
+   per edge.  A resident walk then moves along an edge with one random gather
+   instead of two (the record of the vertex it stands on comes with the edge
+   that led there).  Walks, counts and top-k lists are the same either way.
+   No counterpart in the reference, whose graph is the plain CSR
+   (graphwalker.hpp:168-209 loads beg_pos and csr only).
+   OFF frees them; ON builds them (GW_E_NOMEM if the device lacks the room);
+   AUTO, the default of a resident graph, builds them when they take at most
+   half of the free device memory (environment GW_EDGE_RECORDS=0 makes OFF
+   the default).  Streamed residency drops them; a return to HBM residency
+   applies the mode again.  *built (may be NULL) = 1 when they are in use.   */
+#define GW_EDGE_RECORDS_OFF 0u
+#define GW_EDGE_RECORDS_ON 1u
+#define GW_EDGE_RECORDS_AUTO 2u
+gw_status gw_set_edge_records(gw_ctx *ctx, uint32_t mode, uint32_t *built);
+
 /* ---- measurement -------------------------------------------------------- */
 /* Random 32-byte-sector gather microbenchmark over d_buf (n_words uint32):
    `loads` dependent-free random 4-byte loads; result in *sectors_per_s.     */

@@ -38,8 +38,9 @@ def _oracle_queries(oracle, rp, ci, sources, budgets, rule, L, seed, k):
     return out_ids, out_cnt
 
 
-@pytest.mark.parametrize("rule,L", [(1, 20), (4, 20), (3, 6)])
-def test_ppr_queries_match_oracle(cuda_device, oracle, rule, L):
+@pytest.mark.parametrize("rule,L", [(1, 20), (4, 20), (3, 6), (0, 8)])
+@pytest.mark.parametrize("layout", [0, 1])
+def test_ppr_queries_match_oracle(cuda_device, oracle, rule, L, layout):
     import graphwalker_b200 as gw
     rp, ci = oracle.rmat_csr(13, 8, seed=21)
     deg = np.diff(rp.astype(np.int64))
@@ -52,6 +53,7 @@ def test_ppr_queries_match_oracle(cuda_device, oracle, rule, L):
     k = 50
     ref_ids, ref_cnt = _oracle_queries(oracle, rp, ci, sources, budgets, rule, L, 13, k)
     with gw.Graph.from_csr(rp, ci, oracle.compute_blocks(rp, 64)) as G:
+        assert G.set_edge_records(layout) == bool(layout)
         p = gw.params(rule, gw.SINK_NONE, L, seed=13)
         for batched in (True, False):
             ids, cnt, st = G.ppr(p, sources, budgets, k=k, batched=batched)
@@ -79,6 +81,10 @@ def test_ppr_batched_equals_plain_at_scale(cuda_device):
         assert tuned in (512, 1024, 1536, 2048)
         it, ct, _ = G.ppr(p, sources, budgets, k=100, batched=True)
         assert np.array_equal(it, ib) and np.array_equal(ct, cb)
+        # the plain CSR layout gives the same lists as the edge records
+        assert G.set_edge_records(gw.EDGE_RECORDS_OFF) is False
+        io, co, _ = G.ppr(p, sources, budgets, k=100, batched=True)
+        assert np.array_equal(io, ib) and np.array_equal(co, cb)
 
 
 def test_ppr_full_tables_are_rerun_exactly(cuda_device, oracle):

@@ -11,11 +11,16 @@ from conftest import golden_runs, load_golden
 pytestmark = pytest.mark.gpu
 
 CASES = ["hand", "rmat10", "rmat13"]
+# both graph layouts of the resident kernels: plain CSR (OFF) and edge records (ON)
+LAYOUTS = [0, 1]
 
 
-def _graph(g, residency=0):
+def _graph(g, residency=0, layout=None):
     import graphwalker_b200 as gw
-    return gw.Graph.from_csr(g["rowptr"], g["colidx"], g["blocks"], residency=residency)
+    G = gw.Graph.from_csr(g["rowptr"], g["colidx"], g["blocks"], residency=residency)
+    if layout is not None:
+        assert G.set_edge_records(layout) == bool(layout)
+    return G
 
 
 def _add_golden_walks(G, g, tag):
@@ -33,10 +38,11 @@ def _pool_order(G, cur):
 
 @pytest.mark.parametrize("case", CASES)
 @pytest.mark.parametrize("aggregate", [False, True])
-def test_counts_match_reference_golden(cuda_device, case, aggregate):
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_counts_match_reference_golden(cuda_device, case, aggregate, layout):
     import graphwalker_b200 as gw
     g = load_golden(case)
-    with _graph(g) as G:
+    with _graph(g, layout=layout) as G:
         for tag in golden_runs(g):
             _add_golden_walks(G, g, tag)
             p = gw.params(int(g[f"{tag}_rule"]), gw.SINK_VERTEX_COUNT, int(g[f"{tag}_L"]),
@@ -46,10 +52,11 @@ def test_counts_match_reference_golden(cuda_device, case, aggregate):
 
 
 @pytest.mark.parametrize("case", CASES)
-def test_paths_and_closure_match_reference_golden(cuda_device, case):
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_paths_and_closure_match_reference_golden(cuda_device, case, layout):
     import graphwalker_b200 as gw
     g = load_golden(case)
-    with _graph(g) as G:
+    with _graph(g, layout=layout) as G:
         for tag in golden_runs(g):
             cur, src, hop = _add_golden_walks(G, g, tag)
             rule, L = int(g[f"{tag}_rule"]), int(g[f"{tag}_L"])
@@ -72,7 +79,8 @@ def test_paths_and_closure_match_reference_golden(cuda_device, case):
 
 
 @pytest.mark.parametrize("rule,L", [(0, 10), (1, 10), (2, 10), (3, 7), (4, 20)])
-def test_rmat16_all_rules_match_oracle(cuda_device, oracle, rule, L):
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_rmat16_all_rules_match_oracle(cuda_device, oracle, rule, L, layout):
     import graphwalker_b200 as gw
     rp, ci = oracle.rmat_csr(16, 16, seed=2)
     blocks = oracle.compute_blocks(rp, 512)
@@ -83,6 +91,7 @@ def test_rmat16_all_rules_match_oracle(cuda_device, oracle, rule, L):
     src = cur.copy()
     ref = oracle.run_walks(rp, ci, cur, ids=ids, src=src, rule=rule, L=L, seed=99, stride=32, closure=True)
     with gw.Graph.from_csr(rp, ci, blocks) as G:
+        assert G.set_edge_records(layout) == bool(layout)
         G.add_walks_at(cur, source=src, ids=ids)
         G.run(gw.params(rule, gw.SINK_VERTEX_COUNT, L, seed=99))
         assert np.array_equal(G.read_counts(), ref["counts"])
