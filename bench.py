@@ -531,7 +531,7 @@ def msppr_arm(args) -> None:
             "accuracy_vs_fp64": acc, "cpu_baseline": cpu,
             "e2e": {"value": args.queries / e2e_s, "unit": "queries/s", "api": "gw_ppr_run (host arrays)",
                     "h2d_bytes_per_step": int(args.queries * 8), "d2h_bytes_per_step": int(args.queries * args.topk * 8)},
-            "gpu_launches": 3, "clocks": clk.summary()}
+            "gpu_launches": int(st.launches) * args.steps, "clocks": clk.summary()}
     G.close()
     print(json.dumps(line), flush=True)
 
