@@ -133,6 +133,7 @@ _SIGS = {
     "gw_set_l2_fetch_granularity": (c_int32, [_P, c_uint32, POINTER(c_uint32)]),
     "gw_set_l2_persisting": (c_int32, [_P, c_uint64]),
     "gw_set_edge_records": (c_int32, [_P, c_uint32, POINTER(c_uint32)]),
+    "gw_simrank_meet": (c_int32, [_P, _P, _P, c_uint32, c_uint32, _P, _P]),
 }
 
 _lib = None

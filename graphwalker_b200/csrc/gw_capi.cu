@@ -426,7 +426,8 @@ gw_status gw_close(gw_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   if (ctx->l2_persist_bytes) gw_set_l2_persisting(ctx, 0);
-  for (gw_devbuf* b : {&ctx->d_rowptr, &ctx->d_colidx, &ctx->d_vrec, &ctx->d_erec, &ctx->d_blocks, &ctx->d_status,
+  for (gw_devbuf* b : {&ctx->d_rowptr, &ctx->d_colidx, &ctx->d_vrec, &ctx->d_erec, &ctx->d_meet, &ctx->d_blocks,
+                       &ctx->d_status,
                        &ctx->d_walks, &ctx->d_words, &ctx->d_ids, &ctx->d_counts, &ctx->d_paths,
                        &ctx->d_plen, &ctx->d_closure, &ctx->d_pool_offsets, &ctx->d_dest,
                        &ctx->d_tile_hist, &ctx->d_tile_off, &ctx->d_totals, &ctx->d_minhop,
@@ -506,6 +507,23 @@ gw_status gw_set_residency(gw_ctx* ctx, uint32_t residency, uint32_t nmblocks) {
   }
   ctx->residency = residency;
   return apply_edge_records(ctx);
+}
+
+gw_status gw_simrank_meet(gw_ctx* ctx, const uint32_t* d_paths_a, const uint32_t* d_paths_b, uint32_t R,
+                          uint32_t L, uint64_t* meet, void* stream) {
+  if (!ctx) return set_thread_error(GW_E_INVALID, "NULL context");
+  if (!meet || (R && L && (!d_paths_a || !d_paths_b))) return ctx->fail(GW_E_INVALID, "gw_simrank_meet: NULL argument");
+  if (R > 65535u * 64u) return ctx->fail(GW_E_INVALID, "gw_simrank_meet: R = %u exceeds 4194240", R);
+  if (L == 0) return GW_OK;
+  GW_CUDA(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  GW_CUDA(ctx, ctx->d_meet.ensure((size_t)L * sizeof(unsigned long long)), "meet alloc");
+  GW_CUDA(ctx, gw::launch_simrank_meet(d_paths_a, d_paths_b, R, L, ctx->d_meet.as<unsigned long long>(), st),
+          "simrank_meet");
+  GW_CUDA(ctx, cudaMemcpyAsync(meet, ctx->d_meet.p, (size_t)L * sizeof(uint64_t), cudaMemcpyDeviceToHost, st),
+          "meet copy");
+  GW_CUDA(ctx, cudaStreamSynchronize(st), "synchronize");
+  return GW_OK;
 }
 
 gw_status gw_set_edge_records(gw_ctx* ctx, uint32_t mode, uint32_t* built) {

@@ -30,6 +30,12 @@ def _ptr(a) -> int | None:
     raise TypeError(f"cannot take a pointer of {type(a)}")
 
 
+def simrank_estimate(meet, R: int, decay: float = 0.8) -> float:
+    """SimRank estimate from first-meeting counts: sum_l meet[l] * decay^l / R^2
+    (the quantity SimRank::computeResult sums, apps/simrank.cpp:71-84)."""
+    return float(sum(int(m) * decay ** l for l, m in enumerate(meet)) / (float(R) * float(R)))
+
+
 def params(rule: int = RULE_JUMP, sink: int = SINK_VERTEX_COUNT, L: int = 10, *, njump: int = 0,
            jump_prob: float = 0.15, seed: int = 42, mode: int = MODE_RESIDENT, path_stride: int = 0,
            max_hops: int = 0, prob: float = 0.2, aggregate: bool = False,
@@ -229,6 +235,13 @@ class Graph:
     def pack_words_device(self, walks, n: int, words, wblocks=None, stream: int | None = None) -> None:
         check(load().gw_pack_words_device(self._h, _ptr(walks), n, _ptr(words), _ptr(wblocks),
                                           stream), self._h)
+
+    def simrank_meet(self, paths_a, paths_b, R: int, L: int, stream: int | None = None) -> np.ndarray:
+        """Per-position first-meeting pair counts of two device path arrays
+        (R rows of L visits; gw_simrank_meet)."""
+        meet = np.zeros(L, np.uint64)
+        check(load().gw_simrank_meet(self._h, _ptr(paths_a), _ptr(paths_b), R, L, _ptr(meet), stream), self._h)
+        return meet
 
     def sync(self, stream: int | None = None) -> None:
         check(load().gw_sync(self._h, stream), self._h)

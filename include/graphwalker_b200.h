@@ -292,6 +292,14 @@ gw_status gw_pack_words_device(gw_ctx *ctx, const gw_walk_rec *d_walks, uint64_t
                                uint64_t *d_words, uint32_t *d_blocks, void *stream);
 /* Synchronises the stream and returns the device status of earlier kernels. */
 gw_status gw_sync(gw_ctx *ctx, void *stream);
+/* SimRank's meeting reduction (replaces the O(R^2 L) host loop of
+   SimRank::computeResult, apps/simrank.cpp:71-84).  d_paths_a / d_paths_b:
+   R walks of L visits each, row-major (walk i = row i), 0xFFFFFFFF = no
+   visit.  meet[L] (host) receives, per position l, the number of pairs
+   (i, j) whose first common vertex is at position l; the app's estimate is
+   sum_l meet[l] * 0.8^l / R^2.  R <= 4194240.  Synchronises the stream.     */
+gw_status gw_simrank_meet(gw_ctx *ctx, const uint32_t *d_paths_a, const uint32_t *d_paths_b, uint32_t R,
+                          uint32_t L, uint64_t *meet, void *stream);
 
 /* One superstep of the blocked engine that allocates no memory.  This entry
    point has no counterpart in the reference (whose engine allocates host

@@ -7,6 +7,7 @@
  */
 #include "gw_oracle.h"
 
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -378,4 +379,25 @@ void gwo_expected_visits(const uint64_t *rowptr, const uint32_t *colidx, uint32_
     }
     free(x);
     free(y);
+}
+
+/* ------------------------------------------------------------------------ */
+/* SimRank meeting reduction: the triple loop of SimRank::computeResult     */
+/* (apps/simrank.cpp:71-84), with the per-level pair counts kept as well.   */
+/* ------------------------------------------------------------------------ */
+float gwo_simrank(const uint32_t *a, const uint32_t *b, uint32_t R, uint32_t L, uint64_t *meet) {
+    float simrank = 0;
+    const uint64_t rr = (uint64_t)R * (uint64_t)R; /* wid_t is 64-bit (datatype.hpp:18) */
+    memset(meet, 0, (size_t)L * sizeof(uint64_t));
+    for (uint64_t i = 0; i < R; ++i)
+        for (uint64_t j = 0; j < R; ++j)
+            for (uint32_t l = 0; l < L; ++l) {
+                const uint32_t x = a[i * L + l];
+                if (x == b[j * L + l] && x != 0xffffffffu) {
+                    simrank += (1.0 / rr) * pow(0.8, l);
+                    meet[l]++;
+                    break;
+                }
+            }
+    return simrank;
 }

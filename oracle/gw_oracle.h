@@ -149,6 +149,15 @@ void gwo_expected_visits(const uint64_t *rowptr, const uint32_t *colidx, uint32_
                          uint32_t src, uint32_t rule, uint32_t L, double alpha,
                          double *out);
 
+/* --- SimRank meeting reduction (apps/simrank.cpp:71-84, computeResult) --- */
+
+/* a and b hold R walks of L visits each (walk i = a[i*L .. i*L+L-1],
+ * 0xFFFFFFFF = no visit).  For every pair (i, j) the first l < L with
+ * a[i*L+l] == b[j*L+l] != 0xFFFFFFFF is counted in meet[l] (meet[L] zeroed
+ * first).  Returns the app's estimate accumulated as the app does: a float
+ * sum over i, then j, of (1.0 / (R*R)) * pow(0.8, l), R*R in 64-bit. */
+float gwo_simrank(const uint32_t *a, const uint32_t *b, uint32_t R, uint32_t L, uint64_t *meet);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,6 +66,7 @@ def lib() -> ctypes.CDLL:
             "gwo_rmat_edge": (None, [c_uint64, c_uint32, c_uint64, c_uint32, c_uint32, c_uint32, P, P]),
             "gwo_rmat_csr": (c_uint64, [c_uint32, c_uint64, c_uint64, c_uint32, c_uint32, c_uint32, P, P]),
             "gwo_expected_visits": (None, [P, P, c_uint32, c_uint32, c_uint32, c_uint32, c_double, P]),
+            "gwo_simrank": (ctypes.c_float, [P, P, c_uint32, c_uint32, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -165,6 +166,16 @@ def expected_visits(rowptr, colidx, src, rule, L, alpha=0.15) -> np.ndarray:
     out = np.zeros(nv, np.float64)
     lib().gwo_expected_visits(_p(rowptr), _p(colidx), nv, src, rule, L, alpha, _p(out))
     return out
+
+
+def simrank(paths_a, paths_b, R, L):
+    """(the app's float estimate, per-level first-meeting pair counts)."""
+    a = np.ascontiguousarray(paths_a, dtype=np.uint32).reshape(-1)
+    b = np.ascontiguousarray(paths_b, dtype=np.uint32).reshape(-1)
+    assert a.size == R * L and b.size == R * L
+    meet = np.zeros(L, np.uint64)
+    est = lib().gwo_simrank(_p(a), _p(b), R, L, _p(meet))
+    return float(est), meet
 
 
 def _chooser_coin(seed: int, superstep: int) -> float:

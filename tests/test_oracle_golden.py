@@ -112,3 +112,26 @@ def test_rmat_generator_properties(oracle):
     # skew: R-MAT(0.57, 0.19, 0.19) concentrates out-degree
     deg = np.diff(rp.astype(np.int64))
     assert deg.max() > 20 * deg.mean()
+
+
+def test_oracle_simrank_is_the_apps_float_loop(oracle):
+    """gwo_simrank restates SimRank::computeResult (apps/simrank.cpp:71-84):
+    its float estimate equals the app's loop run on the reference engine's
+    golden paths, bit for bit, and its meeting counts rebuild that estimate."""
+    g = load_golden("rmat10")
+    R, L = 20, 11
+    gp = g["simrank_paths"]
+    for a, b in [(7, 9), (9, 7), (7, 7)]:
+        fa, fb = gp[a], gp[b]
+        sim = np.float32(0.0)
+        meet = np.zeros(L, np.uint64)
+        for i in range(R):
+            for j in range(R):
+                for l in range(L):
+                    if fa[i * L + l] == fb[j * L + l] and fa[i * L + l] != 0xFFFFFFFF:
+                        sim = np.float32(float(sim) + (1.0 / (R * R)) * 0.8 ** l)
+                        meet[l] += 1
+                        break
+        est, m = oracle.simrank(fa.reshape(R, L), fb.reshape(R, L), R, L)
+        assert np.float32(est) == sim, (a, b)
+        assert np.array_equal(m, meet)
