@@ -481,7 +481,7 @@ def msppr_arm(args) -> None:
     sources, budgets = msppr_queries(rp, args.queries)
     del rp
     p = gw.params(gw.RULE_STOP, gw.SINK_NONE, 20, seed=args.walk_seed)
-    tuned = G.ppr_autotune(p, sources[:256], budgets[:256])
+    tuned, tuned_chunk = G.ppr_autotune(p, sources[:256], budgets[:256])
     for _ in range(max(1, args.warmup)):
         G.ppr(p, sources, budgets, k=args.topk, batched=True)
     runs = []
@@ -521,6 +521,7 @@ def msppr_arm(args) -> None:
                                    f"sources uniform over out-degree>=1, budgets round(10^U(2,5)), stop rule p=0.15, "
                                    f"L<=20, top-{args.topk}",
                        "walks_per_step": int(budgets.sum()), "autotuned_threads_per_sm": tuned,
+                       "autotuned_walks_per_warp_grab": tuned_chunk,
                        "graph_layout": layout},
             "breakdown_ms": {"clear": statistics.median(r[1] for r in runs),
                              "walk": statistics.median(r[2] for r in runs),

@@ -122,7 +122,8 @@ _SIGS = {
     "gw_superstep_static": (c_int32, [_P, POINTER(WalkParams), c_uint32, _P, c_uint64, _P, _P, _P, _P, _P]),
     "gw_ppr_run": (c_int32, [_P, POINTER(WalkParams), _P, _P, c_uint32, c_uint32, c_uint32, _P, _P,
                              POINTER(PprStats)]),
-    "gw_ppr_autotune": (c_int32, [_P, POINTER(WalkParams), _P, _P, c_uint32, POINTER(c_uint32)]),
+    "gw_ppr_autotune": (c_int32, [_P, POINTER(WalkParams), _P, _P, c_uint32, POINTER(c_uint32),
+                                  POINTER(c_uint32)]),
     "gw_expected_visits": (c_int32, [_P, POINTER(WalkParams), c_uint32, _P]),
     "gw_serve_open": (c_int32, [_P, POINTER(WalkParams), POINTER(ServeConfig), POINTER(c_void_p)]),
     "gw_serve_submit": (c_int32, [_P, c_uint32, c_uint32, c_uint32, c_uint64, POINTER(c_uint64)]),

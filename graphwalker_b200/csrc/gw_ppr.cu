@@ -109,6 +109,7 @@ __global__ void __launch_bounds__(kPprThreads)
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t below = (1u << lane) - 1u;  // lanes under this one
   const unsigned long long total = w_end - w_begin;
+  const unsigned long long chunk = qv.chunk ? qv.chunk : kWarpChunk;
   const L2Hints hp = make_hints(a.hints);
   // Every walk visits its source at hop 0: the first walk of each query in
   // this launch adds all of them at once and the walks skip that update.
@@ -126,14 +127,14 @@ __global__ void __launch_bounds__(kPprThreads)
     while (idle && !drained) {
       if (c_next >= c_end) {
         unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(qv.cursor, (unsigned long long)kWarpChunk);
+        if (lane == 0) base = atomicAdd(qv.cursor, chunk);
         base = __shfl_sync(~0u, base, 0);
         if (base >= total) {
           drained = true;
           break;
         }
         c_next = base;
-        c_end = base + kWarpChunk < total ? base + kWarpChunk : total;
+        c_end = base + chunk < total ? base + chunk : total;
       }
       const unsigned long long avail = c_end - c_next;
       if (!busy && __popc(idle & below) < avail) {

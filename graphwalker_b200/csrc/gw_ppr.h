@@ -11,10 +11,11 @@ constexpr uint32_t kTopkBuffer = 1024;  // candidate keys per CTA
 constexpr uint32_t kTopkMaxK = kTopkBuffer - kTopkThreads;
 constexpr uint32_t kTopkUnroll = 8;     // table slots a top-k thread loads at once
 
-// Walks a warp takes from the batch cursor at a time: small enough that the
-// walks in flight stay inside a narrow window of the batch (and of its
-// queries), large enough that the cursor's atomic is not contended (64 and
-// 1024 were both slower at R-MAT scale 26 with 4096 queries).
+// Walks a warp takes from the batch cursor at a time, by default: small
+// enough that the walks in flight stay inside a narrow window of the batch
+// (and of its queries), large enough that the cursor's atomic is not
+// contended (64 and 1024 were both slower at R-MAT scale 26 with 4096
+// queries).  gw_ppr_autotune picks it per context with the launch shape.
 constexpr uint32_t kWarpChunk = 256;
 
 struct QueryView {
@@ -28,6 +29,7 @@ struct QueryView {
   const uint32_t* stream;                  // nq: Philox stream word of query q (NULL = 0)
   unsigned long long* visits;              // total visits counter (may be NULL)
   unsigned long long* cursor;              // batch positions handed out (zeroed by the launcher)
+  uint32_t chunk;                          // walks per cursor grab (0 = kWarpChunk)
   uint32_t nq;
 };
 

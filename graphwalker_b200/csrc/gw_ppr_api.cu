@@ -177,6 +177,7 @@ extern "C" gw_status gw_ppr_run(gw_ctx* ctx, const gw_walk_params* params, const
     if (s == GW_OK) s = upload_set(ctx, &set, k, st);
     if (s != GW_OK) break;
     set.qv.visits = ctx->d_q_visits.as<unsigned long long>();
+    set.qv.chunk = ctx->ppr_chunk;
     const bool b = batched || round > 0;
     cudaError_t e = run_set(ctx, params, a, &set, k, b, b ? ctx->ppr_threads_per_sm : 0, st, ev, &local.launches);
     const uint32_t n = (uint32_t)which.size();
@@ -223,7 +224,8 @@ extern "C" gw_status gw_ppr_run(gw_ctx* ctx, const gw_walk_params* params, const
 }
 
 extern "C" gw_status gw_ppr_autotune(gw_ctx* ctx, const gw_walk_params* params, const uint32_t* sources,
-                                     const uint32_t* budgets, uint32_t nq, uint32_t* threads_per_sm) {
+                                     const uint32_t* budgets, uint32_t nq, uint32_t* threads_per_sm,
+                                     uint32_t* walks_per_chunk) {
   if (!ctx) return GW_E_INVALID;
   if (nq == 0 || !sources || !budgets) return ctx->fail(GW_E_INVALID, "empty sample");
   gw::WalkArgs a;
@@ -245,23 +247,30 @@ extern "C" gw_status gw_ppr_autotune(gw_ctx* ctx, const gw_walk_params* params, 
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const int candidates[] = {512, 1024, 1536, 2048};
+  // launch shape (threads per SM) x walks per cursor grab
+  const int thread_candidates[] = {512, 1024, 1536, 2048};
+  const uint32_t chunk_candidates[] = {64, 128, 256, 512};
   int best = 0;
+  uint32_t best_chunk = gw::kWarpChunk;
   float best_ms = 1e30f;
-  for (int c : candidates) {
-    float ms_sum = 0.f;
-    for (int rep = 0; rep < 3; ++rep) {
-      gw::launch_clear_tables(set.qv.tables, set.slots, st);
-      cudaEventRecord(e0, st);
-      gw::launch_walk_queries((int)params->rule, set.qv, 0, set.walks, ctx->view(), a, ctx->d_status.as<uint32_t>(),
-                              c, st);
-      cudaEventRecord(e1, st);
-      cudaEventSynchronize(e1);
-      if (rep) ms_sum += elapsed(e0, e1);  // the first run warms up
-    }
-    if (ms_sum < best_ms) {
-      best_ms = ms_sum;
-      best = c;
+  for (int c : thread_candidates) {
+    for (uint32_t ch : chunk_candidates) {
+      set.qv.chunk = ch;
+      float ms_sum = 0.f;
+      for (int rep = 0; rep < 3; ++rep) {
+        gw::launch_clear_tables(set.qv.tables, set.slots, st);
+        cudaEventRecord(e0, st);
+        gw::launch_walk_queries((int)params->rule, set.qv, 0, set.walks, ctx->view(), a,
+                                ctx->d_status.as<uint32_t>(), c, st);
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        if (rep) ms_sum += elapsed(e0, e1);  // the first run warms up
+      }
+      if (ms_sum < best_ms) {
+        best_ms = ms_sum;
+        best = c;
+        best_chunk = ch;
+      }
     }
   }
   cudaEventDestroy(e0);
@@ -269,6 +278,8 @@ extern "C" gw_status gw_ppr_autotune(gw_ctx* ctx, const gw_walk_params* params, 
   s = gw::take_status(ctx, st);
   if (s != GW_OK) return s;
   ctx->ppr_threads_per_sm = best;
+  ctx->ppr_chunk = best_chunk;
   if (threads_per_sm) *threads_per_sm = (uint32_t)best;
+  if (walks_per_chunk) *walks_per_chunk = best_chunk;
   return GW_OK;
 }

@@ -256,6 +256,7 @@ bool superstep(gw_server* srv) {
   const size_t head = stage_bytes(n, k) - 8 - 2 * (size_t)n * k * 4;
   cudaError_t e = cudaMemcpyAsync(d.prefix, h.prefix, head, cudaMemcpyHostToDevice, st);
   gw::QueryView qv = make_view(d, srv->tables.as<unsigned long long>(), n);
+  qv.chunk = ctx->ppr_chunk;
   if (e == cudaSuccess)
     e = gw::launch_walk_queries((int)srv->params.rule, qv, 0, acc, ctx->view(), srv->args,
                                 ctx->d_status.as<uint32_t>(), ctx->ppr_threads_per_sm, st);

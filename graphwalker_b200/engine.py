@@ -265,13 +265,15 @@ class Graph:
         check(load().gw_expected_visits(self._h, byref(p), source, _ptr(out)), self._h)
         return out
 
-    def ppr_autotune(self, p: WalkParams, sources, budgets) -> int:
+    def ppr_autotune(self, p: WalkParams, sources, budgets) -> tuple[int, int]:
+        """(threads per SM, walks per cursor grab) chosen for this graph's later
+        batched PPR and serving launches (gw_ppr_autotune)."""
         sources = np.ascontiguousarray(sources, dtype=np.uint32)
         budgets = np.ascontiguousarray(budgets, dtype=np.uint32)
-        out = c_uint32()
-        check(load().gw_ppr_autotune(self._h, byref(p), _ptr(sources), _ptr(budgets), len(sources), byref(out)),
-              self._h)
-        return out.value
+        threads, chunk = c_uint32(), c_uint32()
+        check(load().gw_ppr_autotune(self._h, byref(p), _ptr(sources), _ptr(budgets), len(sources), byref(threads),
+                                     byref(chunk)), self._h)
+        return threads.value, chunk.value
 
     def serve(self, p: WalkParams, k: int = 100, mode: int = _lib.SERVE_BATCHED, table_slots: int = 0,
               max_walks_per_step: int = 0, quantum: int = 0) -> "Server":

@@ -227,10 +227,15 @@ gw_status gw_ppr_run(gw_ctx *ctx, const gw_walk_params *params, const uint32_t *
    power series the Monte Carlo counts estimate (count / walks -> out).      */
 gw_status gw_expected_visits(gw_ctx *ctx, const gw_walk_params *params, uint32_t source, double *out);
 /* Times candidate launch shapes of the batched query kernel on the given
-   queries (a sample of the workload) and keeps the fastest for this
-   context; *threads_per_sm receives the choice.                            */
+   queries (a sample of the workload) -- threads per SM in {512, 1024, 1536,
+   2048} x walks a warp takes per grab of the batch cursor in {64, 128, 256,
+   512} -- and keeps the fastest for this context's later gw_ppr_run and
+   server launches.  The choice does not change any result.  Outputs may be
+   NULL.  (The reference has no tuner; msppr's launch is its OpenMP loop,
+   graphwalker.hpp:257-270.)                                                */
 gw_status gw_ppr_autotune(gw_ctx *ctx, const gw_walk_params *params, const uint32_t *sources,
-                          const uint32_t *budgets, uint32_t nq, uint32_t *threads_per_sm);
+                          const uint32_t *budgets, uint32_t nq, uint32_t *threads_per_sm,
+                          uint32_t *walks_per_chunk);
 
 /* ---- serving PPR queries (continuous batching) --------------------------
    No counterpart in the reference, which runs one batch of sources per

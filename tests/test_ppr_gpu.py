@@ -77,8 +77,8 @@ def test_ppr_batched_equals_plain_at_scale(cuda_device):
         assert np.array_equal(ib, ip) and np.array_equal(cb, cp)
         # the source is visited by every walk at hop 0
         assert np.all(cb[:, 0] >= budgets)
-        tuned = G.ppr_autotune(p, sources[:50], budgets[:50])
-        assert tuned in (512, 1024, 1536, 2048)
+        threads, chunk = G.ppr_autotune(p, sources[:50], budgets[:50])
+        assert threads in (512, 1024, 1536, 2048) and chunk in (64, 128, 256, 512)
         it, ct, _ = G.ppr(p, sources, budgets, k=100, batched=True)
         assert np.array_equal(it, ib) and np.array_equal(ct, cb)
         # the plain CSR layout gives the same lists as the edge records
