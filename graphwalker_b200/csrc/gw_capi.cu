@@ -716,9 +716,13 @@ gw_status gw_run_pools(gw_ctx* ctx, const gw_walk_params* params, const uint64_t
   const uint64_t n = pool_offsets[ctx->nblocks];
   if (n && !words) return ctx->fail(GW_E_INVALID, "words is NULL");
   // Chunks of the host words are copied on the copy stream while the walk
-  // kernel of the previous chunk runs on the compute stream.
-  const uint64_t kChunk = 1ull << 22;
-  const uint64_t nchunks = (n + kChunk - 1) / kChunk;
+  // kernel of the previous chunk runs on the compute stream.  A walk word
+  // crosses PCIe faster than its walk runs, so the chunks start small (the
+  // first kernel waits only for a short copy) and grow by 7/4 each time,
+  // which keeps each copy shorter than the kernel it hides behind.
+  std::vector<uint64_t> chunk_lo{0};
+  for (uint64_t m = 1ull << 19; chunk_lo.back() < n; m += m * 3 / 4) chunk_lo.push_back(std::min(n, chunk_lo.back() + m));
+  const uint64_t nchunks = chunk_lo.size() - 1;
   GW_CUDA(ctx, ctx->d_walks.ensure(n * sizeof(gw_walk_rec)), "walk alloc");
   GW_CUDA(ctx, ctx->d_words.ensure(n * 8), "word alloc");
   if (ids) GW_CUDA(ctx, ctx->d_ids.ensure(n * 4), "id alloc");
@@ -738,14 +742,14 @@ gw_status gw_run_pools(gw_ctx* ctx, const gw_walk_params* params, const uint64_t
   cudaStreamWaitEvent(xs, start_ev, 0);
   cudaError_t e = cudaSuccess;
   for (uint64_t c = 0; c < nchunks && e == cudaSuccess; ++c) {
-    const uint64_t lo = c * kChunk, m = std::min(kChunk, n - lo);
+    const uint64_t lo = chunk_lo[c], m = chunk_lo[c + 1] - lo;
     e = cudaMemcpyAsync(ctx->d_words.as<uint64_t>() + lo, words + lo, m * 8, cudaMemcpyHostToDevice, xs);
     if (e == cudaSuccess && ids)
       e = cudaMemcpyAsync(ctx->d_ids.as<uint32_t>() + lo, ids + lo, m * 4, cudaMemcpyHostToDevice, xs);
     if (e == cudaSuccess) e = cudaEventRecord(ready[c], xs);
   }
   for (uint64_t c = 0; c < nchunks && e == cudaSuccess; ++c) {
-    const uint64_t lo = c * kChunk, m = std::min(kChunk, n - lo);
+    const uint64_t lo = chunk_lo[c], m = chunk_lo[c + 1] - lo;
     e = cudaStreamWaitEvent(cs, ready[c], 0);
     if (e == cudaSuccess)
       e = gw::launch_unpack_pools(ctx->d_words.as<uint64_t>() + lo,
