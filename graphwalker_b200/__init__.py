@@ -10,12 +10,13 @@ from ._lib import (EDGE_RECORDS_AUTO, EDGE_RECORDS_OFF, EDGE_RECORDS_ON, MODE_BL
                    RESIDENT_HBM, RULE_JUMP, RULE_PPR, RULE_PROB,
                    RULE_RESTART, RULE_STOP, SINK_CLOSURE_COUNT, SINK_NONE, SINK_PATH_RECORD,
                    SINK_VERTEX_COUNT, STREAM_PINNED, GwError, WalkParams, WalkRec, load)
-from .engine import Graph, compute_blocks, encode, get_current, get_hop, get_source, params, simrank_estimate
+from .engine import (Graph, compute_blocks, convert_edgelist, encode, get_current, get_hop, get_source, params,
+                     simrank_estimate)
 
 __all__ = [
     "Graph", "GwError", "WalkParams", "WalkRec", "params", "encode", "get_source", "get_current",
     "get_hop", "compute_blocks", "load", "RULE_JUMP", "RULE_STOP", "RULE_PROB", "RULE_RESTART",
     "RULE_PPR", "SINK_NONE", "SINK_VERTEX_COUNT", "SINK_PATH_RECORD", "SINK_CLOSURE_COUNT",
     "MODE_RESIDENT", "MODE_BLOCKED", "RESIDENT_HBM", "STREAM_PINNED", "EDGE_RECORDS_OFF",
-    "EDGE_RECORDS_ON", "EDGE_RECORDS_AUTO", "simrank_estimate",
+    "EDGE_RECORDS_ON", "EDGE_RECORDS_AUTO", "simrank_estimate", "convert_edgelist",
 ]

@@ -55,6 +55,13 @@ class ServeStats(Structure):
                 ("restarts", c_uint64), ("pending", c_uint64), ("active", c_uint64)]
 
 
+class ConvertStats(Structure):
+    _fields_ = [("bytes", c_uint64), ("lines", c_uint64), ("edges", c_uint64), ("nvertices", c_uint32),
+                ("nblocks", c_uint32), ("sorted", c_uint32), ("reserved0", c_uint32), ("ms_read", c_double),
+                ("ms_device", c_double), ("ms_write", c_double), ("ms_total", c_double),
+                ("reserved", c_uint64 * 4)]
+
+
 class PprStats(Structure):
     _fields_ = [("walks", c_uint64), ("table_slots", c_uint64), ("launches", c_uint32), ("reserved", c_uint32),
                 ("ms_clear", c_double), ("ms_walk", c_double), ("ms_topk", c_double), ("ms_total", c_double),
@@ -135,6 +142,7 @@ _SIGS = {
     "gw_set_l2_persisting": (c_int32, [_P, c_uint64]),
     "gw_set_edge_records": (c_int32, [_P, c_uint32, POINTER(c_uint32)]),
     "gw_simrank_meet": (c_int32, [_P, _P, _P, c_uint32, c_uint32, _P, _P]),
+    "gw_convert_edgelist": (c_int32, [c_char_p, c_uint64, c_int32, POINTER(ConvertStats)]),
 }
 
 _lib = None

@@ -6,7 +6,8 @@
 // '#' and '%' lines are comments), drops self-loops, keeps duplicate edges
 // and keeps the file's order of a vertex's out-edges.  The reference requires
 // the file to be sorted by source; here a stable sort by source is applied,
-// which leaves a sorted file unchanged.  Block ranges follow compute_block
+// which leaves a sorted file unchanged.  The parsing runs on the GPU
+// (gw_convert_edgelist).  Block ranges follow compute_block
 // (gw_compute_blocks in the C ABI).
 #ifndef GRAPHWALKER_CONVERSIONS_DEF
 #define GRAPHWALKER_CONVERSIONS_DEF
@@ -25,6 +26,7 @@
 #include <vector>
 
 #include "api/datatype.hpp"
+#include "api/cmdopts.hpp"
 #include "api/filename.hpp"
 #include "api/io.hpp"
 #include "graphwalker_b200.h"
@@ -67,52 +69,18 @@ static inline bid_t find_blockrange(std::string base, unsigned long long blocksi
 }
 
 static inline bid_t convert_to_csr(std::string filename, uint16_t filesize_GB) {
-  FILE* in = fopen(filename.c_str(), "r");
-  if (!in) {
-    logstream(LOG_FATAL) << "Could not load :" << filename << " error: " << strerror(errno) << std::endl;
+  // The text is parsed and grouped on the GPU (gw_convert_edgelist), which
+  // writes the same files as the reference's loop (one CSR file: a 1024 GB
+  // file size never splits them).
+  (void)filesize_GB;
+  gw_convert_stats st;
+  const gw_status s = gw_convert_edgelist(filename.c_str(), 0, get_option_int("gw_device", 0), &st);
+  if (s != GW_OK) {
+    logstream(LOG_FATAL) << "convert_to_csr(" << filename << "): " << gw_last_error(nullptr) << std::endl;
     return 0;
   }
-  std::vector<std::pair<vid_t, vid_t>> edges;
-  vid_t max_vert = 0;
-  char line[1024];
-  while (fgets(line, sizeof line, in)) {
-    if (line[0] == '#' || line[0] == '%') continue;
-    char* t1 = strtok(line, "\t, ");
-    char* t2 = strtok(nullptr, "\t, ");
-    if (!t1 || !t2) {
-      logstream(LOG_FATAL) << "Input file is not in right format. Expecting <from> <to>." << std::endl;
-      return 0;
-    }
-    const vid_t from = (vid_t)atoi(t1), to = (vid_t)atoi(t2);
-    if (from == to) continue;
-    max_vert = std::max(max_vert, std::max(from, to));
-    edges.emplace_back(from, to);
-  }
-  fclose(in);
-  std::stable_sort(edges.begin(), edges.end(),
-                   [](const std::pair<vid_t, vid_t>& a, const std::pair<vid_t, vid_t>& b) { return a.first < b.first; });
-  const uint64_t nv = (uint64_t)max_vert + 1;
-  std::vector<uint64_t> rowptr(nv + 1, 0);
-  std::vector<uint32_t> colidx(edges.size());
-  for (size_t i = 0; i < edges.size(); ++i) {
-    rowptr[edges[i].first + 1]++;
-    colidx[i] = edges[i].second;
-  }
-  for (uint64_t v = 0; v < nv; ++v) rowptr[v + 1] += rowptr[v];
-  const std::string dir = filename + "_GraphWalker/";
-  rm_dir(dir);
-  mkdir(dir.c_str(), 0777);
-  mkdir((dir + "graphinfo/").c_str(), 0777);
-  const std::string f0 = fidname(filename, 0);
-  FILE* o = fopen((f0 + ".beg_pos").c_str(), "wb");
-  fwrite(rowptr.data(), 8, rowptr.size(), o);
-  fclose(o);
-  o = fopen((f0 + ".csr").c_str(), "wb");
-  if (!colidx.empty()) fwrite(colidx.data(), 4, colidx.size(), o);
-  fclose(o);
-  std::ofstream(filerangename(filename, filesize_GB).c_str()) << 0 << std::endl << nv << std::endl;
-  std::ofstream(nverticesname(filename).c_str()) << nv << std::endl;
-  logstream(LOG_INFO) << "nverts = " << nv << ", nedges = " << edges.size() << std::endl;
+  logstream(LOG_INFO) << "nverts = " << st.nvertices << ", nedges = " << st.edges << " (" << st.lines << " lines, "
+                      << st.ms_total << " ms)" << std::endl;
   return 1;
 }
 

@@ -198,6 +198,9 @@ gw_status take_status(gw_ctx* ctx, cudaStream_t stream) {
   return GW_OK;
 }
 
+// Errors of entry points that have no context (gw_last_error(NULL)).
+gw_status thread_error(gw_status code, const std::string& msg) { return set_thread_error(code, msg); }
+
 }  // namespace gw
 
 extern "C" {

@@ -149,6 +149,8 @@ struct gw_ctx {
 };
 
 namespace gw {
+// Records an error of an entry point without a context (gw_last_error(NULL)).
+gw_status thread_error(gw_status code, const std::string& msg);
 // Fills launch constants from the API parameters; validates them.
 gw_status make_walk_args(gw_ctx* ctx, const gw_walk_params* p, WalkArgs* a);
 // Reads and clears the device status word (synchronises ctx->stream).

@@ -129,6 +129,12 @@ cudaError_t launch_build_vrec(const unsigned long long* rowptr, uint32_t nv,
     }                                      \
   } while (0)
 
+cudaError_t launch_rowptr_from_sorted(const unsigned long long* keys, uint64_t n, uint32_t nv,
+                                      unsigned long long* rowptr, uint32_t* colidx, cudaStream_t stream) {
+  rowptr_from_sorted_kernel<<<grid_for(n + 1), 256, 0, stream>>>(keys, n, nv, rowptr, colidx);
+  return cudaGetLastError();
+}
+
 cudaError_t rmat_build_csr(uint32_t scale, uint64_t nedges_raw, uint64_t seed, uint32_t ta,
                            uint32_t tab, uint32_t tabc, unsigned long long** rowptr_out,
                            uint32_t** colidx_out, uint64_t* nedges, cudaStream_t stream) {

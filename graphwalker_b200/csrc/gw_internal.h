@@ -60,6 +60,10 @@ cudaError_t launch_build_erec(const uint32_t* colidx, const unsigned long long* 
 // ---- graph kernels (gw_graph.cu) ----
 cudaError_t launch_build_vrec(const unsigned long long* rowptr, uint32_t nv,
                               unsigned long long* vrec, cudaStream_t stream);
+// rowptr[nv + 1] and colidx[n] of edge keys (source << 32 | target) sorted by
+// source (gw_graph.cu).
+cudaError_t launch_rowptr_from_sorted(const unsigned long long* keys, uint64_t n, uint32_t nv,
+                                      unsigned long long* rowptr, uint32_t* colidx, cudaStream_t stream);
 // R-MAT CSR on the device.  On success *rowptr_out / *colidx_out are new
 // device allocations (cudaMalloc) and *nedges the kept edge count.
 cudaError_t rmat_build_csr(uint32_t scale, uint64_t nedges_raw, uint64_t seed, uint32_t ta,

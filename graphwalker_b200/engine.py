@@ -30,6 +30,14 @@ def _ptr(a) -> int | None:
     raise TypeError(f"cannot take a pointer of {type(a)}")
 
 
+def convert_edgelist(path: str, blocksize_kb: int = 0, device: int = 0) -> _lib.ConvertStats:
+    """Text edge list -> the reference's preprocessed files, on the device
+    (gw_convert_edgelist; convert_if_notexists, conversions.hpp:181-404)."""
+    st = _lib.ConvertStats()
+    check(load().gw_convert_edgelist(str(path).encode(), blocksize_kb, device, byref(st)))
+    return st
+
+
 def simrank_estimate(meet, R: int, decay: float = 0.8) -> float:
     """SimRank estimate from first-meeting counts: sum_l meet[l] * decay^l / R^2
     (the quantity SimRank::computeResult sums, apps/simrank.cpp:71-84)."""

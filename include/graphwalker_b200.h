@@ -338,6 +338,31 @@ gw_status gw_set_l2_fetch_granularity(gw_ctx *ctx, uint32_t bytes, uint32_t *pre
    policy window on the launch).  0 releases the reservation.               */
 gw_status gw_set_l2_persisting(gw_ctx *ctx, uint64_t bytes);
 
+/* ---- graph preprocessing -------------------------------------------------- */
+/* Text edge list -> the reference's preprocessed files, on the device:
+   convert_to_csr + compute_block (convert_if_notexists,
+   src/preprocess/conversions.hpp:181-404).  Writes, after removing any old
+   <path>_GraphWalker/ directory as the reference does:
+   graphinfo/file_0.beg_pos, graphinfo/file_0.csr, filesize_1024GB.filerange,
+   N.nvertices and, when blocksize_kb > 0, blocksize_<KB>KB.blockrange.
+   Lines follow the reference's parser: '#'/'%' comment lines, the first two
+   tokens split on tab, comma or space and read by atoi (the low 32 bits of
+   strtol), self-loops dropped, duplicates kept.  The reference needs the
+   lines grouped by ascending source; here lines are grouped by source with a
+   stable sort, which leaves such a file unchanged.  GW_E_INVALID names the
+   first line the reference rejects (fewer than two tokens), or a line longer
+   than 1023 bytes (which its fgets would split).  The text streams through
+   the device in chunks of whole lines; stats may be NULL.                  */
+typedef struct gw_convert_stats {
+  uint64_t bytes, lines, edges;  /* text bytes, lines read, edges kept       */
+  uint32_t nvertices, nblocks;
+  uint32_t sorted;               /* 1 when the lines were already grouped    */
+  uint32_t reserved0;
+  double ms_read, ms_device, ms_write, ms_total;
+  uint64_t reserved[4];
+} gw_convert_stats;
+gw_status gw_convert_edgelist(const char *path, uint64_t blocksize_kb, int32_t device, gw_convert_stats *stats);
+
 /* ---- graph layout -------------------------------------------------------- */
 /* Edge records: a second copy of the column array in which each edge also
    carries its target's packed (first-edge offset, out-degree) record, 16 bytes

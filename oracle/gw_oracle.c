@@ -401,3 +401,88 @@ float gwo_simrank(const uint32_t *a, const uint32_t *b, uint32_t R, uint32_t L, 
             }
     return simrank;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Text edge list -> CSR: convert_to_csr (conversions.hpp:181-291).          */
+/* ------------------------------------------------------------------------ */
+static int is_delim(char c) { return c == '\t' || c == ',' || c == ' '; }   /* strtok(s, "\t, ") */
+
+/* (vid_t)atoi(token): glibc atoi is (int)strtol(s, NULL, 10); leading
+ * isspace() characters, an optional sign, decimal digits; strtol saturates at
+ * LONG_MAX / LONG_MIN and the int conversion keeps the low 32 bits.  The
+ * token never holds a delimiter, so [b, e) is the whole token. */
+static uint32_t ref_atoi(const char *b, const char *e) {
+    while (b < e && (*b == '\n' || *b == '\v' || *b == '\f' || *b == '\r')) ++b;
+    int neg = 0;
+    if (b < e && (*b == '+' || *b == '-')) { neg = *b == '-'; ++b; }
+    uint64_t v = 0;
+    int over = 0;
+    for (; b < e && *b >= '0' && *b <= '9'; ++b) {
+        if (!over) {
+            if (v > (UINT64_MAX - 9) / 10) over = 1;
+            else v = v * 10 + (uint64_t)(*b - '0');
+        }
+    }
+    int64_t r;
+    if (!neg) r = (over || v > (uint64_t)INT64_MAX) ? INT64_MAX : (int64_t)v;
+    else r = (over || v > (uint64_t)INT64_MAX + 1) ? INT64_MIN : (int64_t)(0 - v);
+    return (uint32_t)(uint64_t)r;
+}
+
+uint64_t gwo_convert_text(const char *text, uint64_t len, uint64_t *rowptr, uint32_t *colidx,
+                          uint32_t *nv_out, uint64_t *ne_out) {
+    uint64_t cap = 1024, ne = 0, lineno = 0;
+    uint32_t *src = (uint32_t *)malloc(cap * 4), *dst = (uint32_t *)malloc(cap * 4);
+    uint32_t max_vert = 0;
+    uint64_t pos = 0, bad = 0;
+    while (pos < len) {
+        /* one fgets line: through '\n' or the end of the text */
+        uint64_t end = pos;
+        while (end < len && text[end] != '\n') ++end;
+        if (end < len) ++end;
+        ++lineno;
+        if (end - pos > 1023) { bad = lineno; break; }
+        const char *s = text + pos, *lim = text + end;
+        pos = end;
+        for (const char *z = s; z < lim; ++z) if (*z == '\0') { lim = z; break; }   /* C string end */
+        if (s < lim && (s[0] == '#' || s[0] == '%')) continue;
+        const char *t1 = s;
+        while (t1 < lim && is_delim(*t1)) ++t1;
+        const char *e1 = t1;
+        while (e1 < lim && !is_delim(*e1)) ++e1;
+        const char *t2 = e1;
+        while (t2 < lim && is_delim(*t2)) ++t2;
+        const char *e2 = t2;
+        while (e2 < lim && !is_delim(*e2)) ++e2;
+        if (t1 == e1 || t2 == e2) { bad = lineno; break; }
+        const uint32_t from = ref_atoi(t1, e1), to = ref_atoi(t2, e2);
+        if (from == to) continue;                       /* conversions.hpp:239 */
+        if (from > max_vert) max_vert = from;
+        if (to > max_vert) max_vert = to;
+        if (ne == cap) {
+            cap *= 2;
+            src = (uint32_t *)realloc(src, cap * 4);
+            dst = (uint32_t *)realloc(dst, cap * 4);
+        }
+        src[ne] = from;
+        dst[ne] = to;
+        ++ne;
+    }
+    if (!bad) {
+        const uint64_t nv = (uint64_t)max_vert + 1;
+        if (nv_out) *nv_out = (uint32_t)nv;
+        if (ne_out) *ne_out = ne;
+        if (rowptr && colidx) {   /* stable counting sort by source */
+            memset(rowptr, 0, (nv + 1) * sizeof(uint64_t));
+            for (uint64_t i = 0; i < ne; ++i) rowptr[src[i] + 1]++;
+            for (uint64_t v = 0; v < nv; ++v) rowptr[v + 1] += rowptr[v];
+            uint64_t *fill = (uint64_t *)malloc(nv * sizeof(uint64_t));
+            memcpy(fill, rowptr, nv * sizeof(uint64_t));
+            for (uint64_t i = 0; i < ne; ++i) colidx[fill[src[i]]++] = dst[i];
+            free(fill);
+        }
+    }
+    free(src);
+    free(dst);
+    return bad;
+}

@@ -149,6 +149,21 @@ void gwo_expected_visits(const uint64_t *rowptr, const uint32_t *colidx, uint32_
                          uint32_t src, uint32_t rule, uint32_t L, double alpha,
                          double *out);
 
+/* --- text edge list -> CSR (src/preprocess/conversions.hpp:181-291) --- */
+
+/* The reference's convert_to_csr on text[0, len): lines as fgets reads them,
+ * '#'/'%' comment lines skipped, the first two strtok tokens (delimiters tab,
+ * comma, space) converted by atoi into vid_t (the low 32 bits of strtol),
+ * self-loops dropped, duplicates kept.  Lines are grouped by source with a
+ * stable sort (the reference expects them grouped already, in which case
+ * the sort changes nothing).  nv = largest vertex id seen + 1 (1 when there
+ * are no edges).  With rowptr/colidx NULL only *nv and *ne are computed;
+ * otherwise rowptr[nv + 1] and colidx[ne] are filled.  Returns 0, or the
+ * 1-based number of the first line the reference rejects (fewer than two
+ * tokens) or that is longer than 1023 bytes (fgets would split it). */
+uint64_t gwo_convert_text(const char *text, uint64_t len, uint64_t *rowptr, uint32_t *colidx,
+                          uint32_t *nv, uint64_t *ne);
+
 /* --- SimRank meeting reduction (apps/simrank.cpp:71-84, computeResult) --- */
 
 /* a and b hold R walks of L visits each (walk i = a[i*L .. i*L+L-1],

@@ -67,6 +67,7 @@ def lib() -> ctypes.CDLL:
             "gwo_rmat_csr": (c_uint64, [c_uint32, c_uint64, c_uint64, c_uint32, c_uint32, c_uint32, P, P]),
             "gwo_expected_visits": (None, [P, P, c_uint32, c_uint32, c_uint32, c_uint32, c_double, P]),
             "gwo_simrank": (ctypes.c_float, [P, P, c_uint32, c_uint32, P]),
+            "gwo_convert_text": (c_uint64, [ctypes.c_char_p, c_uint64, P, P, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -166,6 +167,19 @@ def expected_visits(rowptr, colidx, src, rule, L, alpha=0.15) -> np.ndarray:
     out = np.zeros(nv, np.float64)
     lib().gwo_expected_visits(_p(rowptr), _p(colidx), nv, src, rule, L, alpha, _p(out))
     return out
+
+
+def convert_text(text: bytes):
+    """(rowptr u64[nv+1], colidx u32[ne]) as convert_to_csr builds them;
+    raises ValueError naming the first line the reference rejects."""
+    nv, ne = ctypes.c_uint32(), ctypes.c_uint64()
+    bad = lib().gwo_convert_text(text, len(text), None, None, ctypes.byref(nv), ctypes.byref(ne))
+    if bad:
+        raise ValueError(f"line {bad} is not '<from> <to>' (or exceeds 1023 bytes)")
+    rowptr = np.zeros(nv.value + 1, np.uint64)
+    colidx = np.zeros(max(ne.value, 1), np.uint32)
+    lib().gwo_convert_text(text, len(text), _p(rowptr), _p(colidx), None, None)
+    return rowptr, colidx[: ne.value]
 
 
 def simrank(paths_a, paths_b, R, L):

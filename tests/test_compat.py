@@ -139,3 +139,24 @@ def test_unchanged_rwdomination_graphlet_kkppr_apps(cuda_device, tmp_path):
     assert r.returncode == 0, r.stderr[-2000:]
     r = _run_app("rawrandomwalks", ["file", base, "N", "1024", "R", "3000", "L", "6", "blocksize_kb", kb], tmp_path)
     assert r.returncode == 0, r.stderr[-2000:]
+
+
+@pytest.mark.gpu
+def test_unchanged_app_preprocesses_a_text_edge_list(cuda_device, tmp_path):
+    """apps/rwdomination.cpp, unchanged, given a text edge list with no
+    preprocessed files: its convert_if_notexists call runs the GPU converter,
+    which writes exactly the files the reference's preprocessor writes."""
+    gold = np.load(ROOT / "tests" / "golden" / "convert.npz")
+    (tmp_path / "conf").mkdir()
+    (tmp_path / "conf" / "graphwalker.cnf").write_text("# empty\n")
+    text = tmp_path / "g.txt"
+    text.write_bytes(gold["rmat10_text"].tobytes())
+    kb = int(gold["blocksize_kb"])
+    r = _run_app("rwdomination", ["file", str(text), "N", "1024", "R", "1", "L", "5", "blocksize_kb", str(kb)],
+                 tmp_path)
+    assert r.returncode == 0, r.stderr[-2000:]
+    d = Path(str(text) + "_GraphWalker")
+    assert np.array_equal(np.fromfile(d / "graphinfo" / "file_0.beg_pos", np.uint64), gold["rmat10_beg_pos"])
+    assert np.array_equal(np.fromfile(d / "graphinfo" / "file_0.csr", np.uint32), gold["rmat10_csr"])
+    br = np.array((d / f"blocksize_{kb}KB.blockrange").read_text().split(), np.uint32)
+    assert np.array_equal(br, gold["rmat10_blockrange"])

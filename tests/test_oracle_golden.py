@@ -1,6 +1,8 @@
 """Pins the C oracle to the reference: golden vectors made by GraphWalker's
 own engine and walk classes (tests/golden/make_golden.py), the published
 Philox4x32-10 known-answer vectors, and the float continuation test."""
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -135,3 +137,27 @@ def test_oracle_simrank_is_the_apps_float_loop(oracle):
         est, m = oracle.simrank(fa.reshape(R, L), fb.reshape(R, L), R, L)
         assert np.float32(est) == sim, (a, b)
         assert np.array_equal(m, meet)
+
+
+def test_oracle_converter_is_the_references(oracle):
+    """gwo_convert_text restates convert_to_csr (conversions.hpp:181-291): on
+    every golden edge list it builds the row pointer and column array the
+    reference's own preprocessor wrote, and compute_blocks gives its block
+    range (compute_block, conversions.hpp:293-359)."""
+    g = np.load(Path(__file__).parent / "golden" / "convert.npz")
+    kb = int(g["blocksize_kb"])
+    for case in g["cases"]:
+        rp, ci = oracle.convert_text(g[f"{case}_text"].tobytes())
+        assert np.array_equal(rp, g[f"{case}_beg_pos"]), case
+        assert np.array_equal(ci, g[f"{case}_csr"]), case
+        assert g[f"{case}_nvertices"].tobytes() == f"{len(rp) - 1}\n".encode()
+        assert np.array_equal(oracle.compute_blocks(rp, kb), g[f"{case}_blockrange"]), case
+
+
+@pytest.mark.parametrize("text,line", [(b"0 1\n\n1 2\n", 2), (b"0 1\n7\n", 2), (b"0 1\r\n\r\n", 2),
+                                       (b"# x\n" + b"1 " * 600 + b"\n", 2)])
+def test_oracle_converter_rejects_what_the_reference_rejects(oracle, text, line):
+    """An empty line or a one-token line has no second token (the reference
+    asserts, conversions.hpp:226-233); an over-long line would be split by fgets."""
+    with pytest.raises(ValueError, match=f"line {line} "):
+        oracle.convert_text(text)
