@@ -69,13 +69,14 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-probe", action="store_true", help="skip the random-gather roof probe")
     ap.add_argument("--cpu-sample-sec", type=float, default=15.0)
-    ap.add_argument("--workload", choices=["rawwalk", "msppr", "serve", "ppr1", "ooc"], default="rawwalk",
+    ap.add_argument("--workload", choices=["rawwalk", "msppr", "serve", "ppr1", "ooc", "convert"], default="rawwalk",
                     help="rawwalk: the headline raw-random-walk step; msppr: batched vs plain multi-source PPR; "
                          "serve: Poisson-arrival PPR serving, continuous batching vs one query per launch")
     ap.add_argument("--rates", default="1000,5000,10000,20000,50000", help="serve: arrival rates (queries/s)")
     ap.add_argument("--serve-sec", type=float, default=2.0, help="serve: seconds of arrivals per rate")
     ap.add_argument("--nmblocks", type=int, default=32, help="ooc: device block slots")
     ap.add_argument("--queries", type=int, default=4096)
+    ap.add_argument("--convert-sample-mb", type=int, default=512, help="convert: text prefix the reference parses")
     ap.add_argument("--topk", type=int, default=100)
     return ap.parse_args()
 
@@ -701,8 +702,107 @@ def ooc_arm(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def edge_list_text(src, dst) -> "np.ndarray":
+    """'<src> <dst>\n' lines of two CUDA integer tensors, formatted on the GPU
+    (input preparation for the convert workload); returns host bytes as uint8."""
+    import torch
+    s, d = src.to(torch.int64), dst.to(torch.int64)
+
+    def ndigits(x):
+        n = torch.ones_like(x)
+        p = 10
+        for _ in range(9):
+            n += (x >= p).to(torch.int64)
+            p *= 10
+        return n
+
+    ns, nd = ndigits(s), ndigits(d)
+    end = torch.cumsum(ns + nd + 2, 0)
+    start = end - (ns + nd + 2)
+    buf = torch.full((int(end[-1].item()),), 32, dtype=torch.uint8, device=s.device)
+    for k in range(10):
+        p10 = 10 ** k
+        m = ns > k
+        buf[start[m] + ns[m] - 1 - k] = (48 + (s[m] // p10) % 10).to(torch.uint8)
+        m = nd > k
+        buf[start[m] + ns[m] + nd[m] - k] = (48 + (d[m] // p10) % 10).to(torch.uint8)
+    buf[end - 1] = 10
+    return buf.cpu().numpy()
+
+
+def convert_arm(args) -> None:
+    """Graph preprocessing: a text edge list (an R-MAT graph, lines grouped by
+    source as the reference requires) to the reference's preprocessed files,
+    on the device (gw_convert_edgelist) against the reference's own
+    convert_if_notexists compiled from source on a prefix of the same text."""
+    import numpy as np
+    import torch
+
+    import graphwalker_b200 as gw
+    torch.cuda.set_device(0)
+    scale = args.scale if args.scale != 24 else 23
+    kb = blocksize_kb_for(scale, args.edge_factor, args.nblocks)
+    with gw.Graph.rmat(scale, args.edge_factor, seed=args.graph_seed, blocksize_kb=kb) as G:
+        rp, ci = G.export_csr()
+    src = torch.repeat_interleave(torch.arange(len(rp) - 1, device="cuda"),
+                                  torch.from_numpy(np.diff(rp.astype(np.int64))).cuda())
+    text = edge_list_text(src, torch.from_numpy(ci.astype(np.int64)).cuda())
+    del src
+    torch.cuda.empty_cache()
+    ne = len(ci)
+    with tempfile.TemporaryDirectory(prefix="gw_conv_") as td:
+        path = Path(td) / "rmat.txt"
+        text.tofile(path)
+        runs = []
+        for _ in range(max(1, args.warmup) + max(1, args.steps)):
+            runs.append(gw.convert_edgelist(str(path), kb))
+        timed = runs[max(1, args.warmup):]
+        st = sorted(timed, key=lambda r: r.ms_total)[len(timed) // 2]
+        out_dir = Path(str(path) + "_GraphWalker")
+        # the text names vertices up to its largest id; the generator's row pointer continues flat after it
+        got_rp = np.fromfile(out_dir / "graphinfo" / "file_0.beg_pos", np.uint64)
+        ok_full = (np.array_equal(got_rp, rp[: len(got_rp)]) and bool(np.all(rp[len(got_rp):] == ne))
+                   and np.array_equal(np.fromfile(out_dir / "graphinfo" / "file_0.csr", np.uint32), ci))
+        # the reference on a prefix of whole lines (a bounded sample), ours on the same prefix
+        cpu, same = None, None
+        if not args.no_cpu_baseline:
+            exe = ROOT / "oracle" / "_ref" / "gw_ref_convert"
+            cut = int(min(len(text), args.convert_sample_mb << 20))
+            cut = int(np.flatnonzero(text[:cut] == 10)[-1]) + 1
+            sample = Path(td) / "sample.txt"
+            text[:cut].tofile(sample)
+            ref = Path(td) / "sample_ref.txt"
+            os.link(sample, ref)
+            t0 = time.perf_counter()
+            subprocess.run([str(exe), str(ref), str(kb)], check=True, capture_output=True)
+            ref_s = time.perf_counter() - t0
+            mine = gw.convert_edgelist(str(sample), kb)
+            a, b = Path(str(sample) + "_GraphWalker"), Path(str(ref) + "_GraphWalker")
+            same = all((a / f).read_bytes() == (b / f).read_bytes()
+                       for f in ("graphinfo/file_0.beg_pos", "graphinfo/file_0.csr", "N.nvertices",
+                                 "filesize_1024GB.filerange", f"blocksize_{kb}KB.blockrange"))
+            cpu = {"value": mine.edges / ref_s, "unit": "edges/s", "cores": 1, "kind": "reference",
+                   "sample": f"the reference's convert_if_notexists (conversions.hpp) compiled -O3 from source, "
+                             f"single-threaded as written, on the first {cut} bytes ({mine.lines} lines) of the "
+                             f"same text; {ref_s:.2f} s"}
+    line = {"metric": "edges/s", "value": ne / (st.ms_total * 1e-3), "unit": "edges/s", "workload": "convert",
+            "n_gpus": 1, "steps": max(1, args.steps), "warmup": max(1, args.warmup), "ms_per_step": st.ms_total,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": f"text edge list -> preprocessed CSR + block range, R-MAT scale {scale} "
+                                   f"ef {args.edge_factor} ({len(text)} bytes, {ne} lines, grouped by source), "
+                                   f"blocksize {kb} KB; the text file is in the page cache"},
+            "text_GBps": len(text) / (st.ms_total * 1e-3) / 1e9,
+            "breakdown_ms": {"read": st.ms_read, "device": st.ms_device, "write": st.ms_write},
+            "identical_to_generator_csr": bool(ok_full), "identical_to_reference_on_sample": same,
+            "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.workload == "convert" and args.impl != "reference":
+        convert_arm(args)
+        return
     if args.workload == "ooc" and args.impl != "reference":
         ooc_arm(args)
         return
