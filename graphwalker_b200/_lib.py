@@ -142,6 +142,7 @@ _SIGS = {
     "gw_set_l2_persisting": (c_int32, [_P, c_uint64]),
     "gw_set_edge_records": (c_int32, [_P, c_uint32, POINTER(c_uint32)]),
     "gw_simrank_meet": (c_int32, [_P, _P, _P, c_uint32, c_uint32, _P, _P]),
+    "gw_simrank_batch": (c_int32, [_P, POINTER(WalkParams), _P, _P, c_uint32, c_uint32, c_double, _P, _P]),
     "gw_convert_edgelist": (c_int32, [c_char_p, c_uint64, c_int32, POINTER(ConvertStats)]),
 }
 

@@ -429,7 +429,7 @@ gw_status gw_close(gw_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   if (ctx->l2_persist_bytes) gw_set_l2_persisting(ctx, 0);
-  for (gw_devbuf* b : {&ctx->d_rowptr, &ctx->d_colidx, &ctx->d_vrec, &ctx->d_erec, &ctx->d_meet, &ctx->d_blocks,
+  for (gw_devbuf* b : {&ctx->d_rowptr, &ctx->d_colidx, &ctx->d_vrec, &ctx->d_erec, &ctx->d_meet, &ctx->d_sr_rows, &ctx->d_blocks,
                        &ctx->d_status,
                        &ctx->d_walks, &ctx->d_words, &ctx->d_ids, &ctx->d_counts, &ctx->d_paths,
                        &ctx->d_plen, &ctx->d_closure, &ctx->d_pool_offsets, &ctx->d_dest,
@@ -521,11 +521,86 @@ gw_status gw_simrank_meet(gw_ctx* ctx, const uint32_t* d_paths_a, const uint32_t
   GW_CUDA(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   GW_CUDA(ctx, ctx->d_meet.ensure((size_t)L * sizeof(unsigned long long)), "meet alloc");
-  GW_CUDA(ctx, gw::launch_simrank_meet(d_paths_a, d_paths_b, R, L, ctx->d_meet.as<unsigned long long>(), st),
+  GW_CUDA(ctx, gw::launch_simrank_meet(d_paths_a, d_paths_b, nullptr, 1, R, L, ctx->d_meet.as<unsigned long long>(),
+                                       st),
           "simrank_meet");
   GW_CUDA(ctx, cudaMemcpyAsync(meet, ctx->d_meet.p, (size_t)L * sizeof(uint64_t), cudaMemcpyDeviceToHost, st),
           "meet copy");
   GW_CUDA(ctx, cudaStreamSynchronize(st), "synchronize");
+  return GW_OK;
+}
+
+gw_status gw_simrank_batch(gw_ctx* ctx, const gw_walk_params* params, const uint32_t* a, const uint32_t* b,
+                           uint32_t nq, uint32_t R, double decay, uint64_t* meet, double* scores) {
+  if (!ctx) return set_thread_error(GW_E_INVALID, "NULL context");
+  if (!params || (nq && (!a || !b || !scores))) return ctx->fail(GW_E_INVALID, "gw_simrank_batch: NULL argument");
+  if (params->rule != GW_RULE_RESTART)
+    return ctx->fail(GW_E_INVALID, "SimRank walks use the restart rule (RandomWalkwithRestartwithJoint)");
+  if (ctx->residency != GW_RESIDENT_HBM) return ctx->fail(GW_E_STATE, "gw_simrank_batch needs a resident graph");
+  const uint32_t L = params->L;
+  if (L == 0 || R == 0 || R > 65535u * 64u || nq > (1u << 31))
+    return ctx->fail(GW_E_INVALID, "gw_simrank_batch: need L > 0, 0 < R <= 4194240, nq <= 2^31");
+  if (nq == 0) return GW_OK;
+  gw_walk_params pp = *params;  // the walks record their paths, L positions per replica
+  pp.sink = GW_SINK_PATH_RECORD;
+  pp.path_stride = L;
+  gw::WalkArgs wa;
+  gw_status s = gw::make_walk_args(ctx, &pp, &wa);
+  if (s != GW_OK) return s;
+  // the distinct vertices of the batch, R walks each (the app's placement, simrank.cpp:30-57)
+  std::vector<uint32_t> verts(a, a + nq);
+  verts.insert(verts.end(), b, b + nq);
+  std::sort(verts.begin(), verts.end());
+  verts.erase(std::unique(verts.begin(), verts.end()), verts.end());
+  for (uint32_t v : verts)
+    if (v >= ctx->nv) return ctx->fail(GW_E_INVALID, "SimRank vertex %u >= nvertices", v);
+  const uint64_t n = (uint64_t)verts.size() * R;
+  if ((uint64_t)(R - 1) * L >= (1ull << 32)) return ctx->fail(GW_E_INVALID, "R * L exceeds the 32-bit hop field");
+  std::vector<gw_walk_rec> recs(n);
+  for (size_t k = 0; k < verts.size(); ++k)
+    for (uint32_t i = 0; i < R; ++i) recs[k * R + i] = gw_walk_rec{verts[k], verts[k], verts[k], i * L};
+  std::vector<unsigned long long> rows(2 * (size_t)nq);
+  auto row_of = [&](uint32_t v) {
+    return (unsigned long long)(std::lower_bound(verts.begin(), verts.end(), v) - verts.begin()) * R * L;
+  };
+  for (uint32_t q = 0; q < nq; ++q) {
+    rows[2 * q] = row_of(a[q]);
+    rows[2 * q + 1] = row_of(b[q]);
+  }
+  GW_CUDA(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  cudaStream_t st = ctx->stream;
+  GW_CUDA(ctx, ctx->d_walks.ensure(n * sizeof(gw_walk_rec)), "walk alloc");
+  GW_CUDA(ctx, ctx->d_paths.ensure(n * L * 4), "paths alloc");
+  GW_CUDA(ctx, ctx->d_plen.ensure(n * 4), "plen alloc");
+  GW_CUDA(ctx, ctx->d_sr_rows.ensure(rows.size() * 8), "rows alloc");
+  GW_CUDA(ctx, ctx->d_meet.ensure((size_t)nq * L * 8), "meet alloc");
+  GW_CUDA(ctx, cudaMemcpyAsync(ctx->d_walks.p, recs.data(), n * sizeof(gw_walk_rec), cudaMemcpyHostToDevice, st),
+          "walk upload");
+  GW_CUDA(ctx, cudaMemcpyAsync(ctx->d_sr_rows.p, rows.data(), rows.size() * 8, cudaMemcpyHostToDevice, st),
+          "rows upload");
+  GW_CUDA(ctx, cudaMemsetAsync(ctx->d_paths.p, 0xff, n * L * 4, st), "paths clear");
+  gw::SinkView sv{};
+  sv.paths = ctx->d_paths.as<uint32_t>();
+  sv.plen = ctx->d_plen.as<uint32_t>();
+  GW_CUDA(ctx, gw::launch_walk_resident(GW_RULE_RESTART, GW_SINK_PATH_RECORD, false, ctx->d_walks.as<gw_walk_rec>(),
+                                        n, ctx->view(), wa, sv, ctx->d_status.as<uint32_t>(), 0, st, nullptr),
+          "simrank walks");
+  GW_CUDA(ctx, gw::launch_simrank_meet(ctx->d_paths.as<uint32_t>(), ctx->d_paths.as<uint32_t>(),
+                                       ctx->d_sr_rows.as<unsigned long long>(), nq, R, L,
+                                       ctx->d_meet.as<unsigned long long>(), st),
+          "simrank meet");
+  std::vector<uint64_t> m((size_t)nq * L);
+  GW_CUDA(ctx, cudaMemcpyAsync(m.data(), ctx->d_meet.p, m.size() * 8, cudaMemcpyDeviceToHost, st), "meet copy");
+  s = gw::take_status(ctx, st);  // synchronises the stream
+  if (s != GW_OK) return s;
+  const double rr = (double)R * (double)R;
+  for (uint32_t q = 0; q < nq; ++q) {
+    double sc = 0.0, w = 1.0;
+    for (uint32_t l = 0; l < L; ++l, w *= decay) sc += (double)m[(size_t)q * L + l] * w;
+    scores[q] = sc / rr;
+  }
+  if (meet) std::copy(m.begin(), m.end(), meet);
+  ctx->have_run = false;  // the path buffers now hold SimRank walks, not a gw_run's
   return GW_OK;
 }
 

@@ -70,7 +70,7 @@ struct gw_ctx {
   std::vector<uint32_t> blocks;  // nblocks + 1
   gw_devbuf d_rowptr, d_colidx, d_vrec, d_blocks;
   gw_devbuf d_erec;                     // edge records (empty = not built)
-  gw_devbuf d_meet;                     // SimRank meeting counts
+  gw_devbuf d_meet, d_sr_rows;          // SimRank meeting counts, per-query path rows
   uint32_t erec_mode = GW_EDGE_RECORDS_AUTO;
   gw_hostbuf h_rowptr, h_colidx;  // pinned copy (streaming residency)
 

@@ -50,9 +50,11 @@ cudaError_t launch_unpack_pools(const uint64_t* words, const uint32_t* ids, uint
 cudaError_t launch_pack_words(const gw_walk_rec* walks, uint64_t n, const uint32_t* blocks,
                               uint32_t nblocks, uint64_t* words, uint32_t* wblock,
                               cudaStream_t stream);
-// SimRank meeting counts meet[L] of two R x L path arrays (gw_simrank.cu).
-cudaError_t launch_simrank_meet(const uint32_t* a, const uint32_t* b, uint32_t R, uint32_t L,
-                                unsigned long long* meet, cudaStream_t stream);
+// SimRank meeting counts meet[q * L + l] of nq queries: query q compares the
+// R x L path rows at element offset rows[2q] of a with rows[2q + 1] of b
+// (rows NULL: one query at offset 0 of both) (gw_simrank.cu).
+cudaError_t launch_simrank_meet(const uint32_t* a, const uint32_t* b, const unsigned long long* rows, uint32_t nq,
+                                uint32_t R, uint32_t L, unsigned long long* meet, cudaStream_t stream);
 // erec[e] = (packed record of colidx[e], colidx[e]) for e < ne (gw_walk.cu).
 cudaError_t launch_build_erec(const uint32_t* colidx, const unsigned long long* vrec, uint64_t ne, uint32_t nv,
                               ulonglong2* erec, cudaStream_t stream);

@@ -9,6 +9,8 @@
 // two tiles' visits are staged in shared memory 32 positions at a time, each
 // thread owns a 4 x 4 block of pairs and keeps their "met" flags in a 16-bit
 // mask, so positions beyond a pair's first meeting are skipped by masking.
+// The grid's z dimension runs over queries: query q compares the R walks at
+// row offset rows[2q] of `a` with those at rows[2q + 1] of `b`.
 #include "gw_internal.h"
 
 namespace gw {
@@ -20,11 +22,16 @@ constexpr int kSrChunk = 32;     // positions staged at a time
 constexpr int kSrThreads = 256;  // 16 x 16 threads, 4 x 4 pairs each
 
 __global__ void __launch_bounds__(kSrThreads)
-    simrank_meet_kernel(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b, uint32_t R, uint32_t L,
-                        unsigned long long* __restrict__ meet) {
+    simrank_meet_kernel(const uint32_t* __restrict__ a0, const uint32_t* __restrict__ b0,
+                        const unsigned long long* __restrict__ rows, uint32_t q0, uint32_t R, uint32_t L,
+                        unsigned long long* __restrict__ meet0) {
   __shared__ uint32_t sa[kSrChunk][kSrTile + 1];
   __shared__ uint32_t sb[kSrChunk][kSrTile + 1];
   __shared__ uint32_t hist[kSrChunk];
+  const uint32_t q = q0 + blockIdx.z;
+  const uint32_t* __restrict__ a = a0 + (rows ? rows[2 * (size_t)q] : 0ull);
+  const uint32_t* __restrict__ b = b0 + (rows ? rows[2 * (size_t)q + 1] : 0ull);
+  unsigned long long* __restrict__ meet = meet0 + (size_t)q * L;
   const uint32_t i0 = blockIdx.y * kSrTile, j0 = blockIdx.x * kSrTile;
   const uint32_t tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   uint32_t met = 0;  // bit u * 4 + w: pair (i0 + ty + 16u, j0 + tx + 16w) has met
@@ -65,13 +72,17 @@ __global__ void __launch_bounds__(kSrThreads)
 
 }  // namespace
 
-cudaError_t launch_simrank_meet(const uint32_t* a, const uint32_t* b, uint32_t R, uint32_t L,
-                                unsigned long long* meet, cudaStream_t stream) {
-  cudaError_t e = cudaMemsetAsync(meet, 0, (size_t)L * sizeof(unsigned long long), stream);
+cudaError_t launch_simrank_meet(const uint32_t* a, const uint32_t* b, const unsigned long long* rows, uint32_t nq,
+                                uint32_t R, uint32_t L, unsigned long long* meet, cudaStream_t stream) {
+  cudaError_t e = cudaMemsetAsync(meet, 0, (size_t)nq * L * sizeof(unsigned long long), stream);
   if (e != cudaSuccess || R == 0 || L == 0) return e;
   const uint32_t tiles = (R + kSrTile - 1) / kSrTile;
-  simrank_meet_kernel<<<dim3(tiles, tiles), kSrThreads, 0, stream>>>(a, b, R, L, meet);
-  return cudaGetLastError();
+  for (uint32_t q0 = 0; q0 < nq && e == cudaSuccess; q0 += 65535u) {
+    const uint32_t nz = nq - q0 < 65535u ? nq - q0 : 65535u;
+    simrank_meet_kernel<<<dim3(tiles, tiles, nz), kSrThreads, 0, stream>>>(a, b, rows, q0, R, L, meet);
+    e = cudaGetLastError();
+  }
+  return e;
 }
 
 }  // namespace gw

@@ -251,6 +251,19 @@ class Graph:
         check(load().gw_simrank_meet(self._h, _ptr(paths_a), _ptr(paths_b), R, L, _ptr(meet), stream), self._h)
         return meet
 
+    def simrank_batch(self, a, b, R: int, L: int, seed: int = 42, decay: float = 0.8):
+        """SimRank estimates of the queries (a[q], b[q]) and their per-position
+        first-meeting counts (gw_simrank_batch): scores float64[nq], meet uint64[nq, L]."""
+        a = np.ascontiguousarray(a, dtype=np.uint32)
+        b = np.ascontiguousarray(b, dtype=np.uint32)
+        nq = len(a)
+        scores = np.zeros(nq, np.float64)
+        meet = np.zeros((nq, L), np.uint64)
+        p = params(_lib.RULE_RESTART, _lib.SINK_PATH_RECORD, L, seed=seed)
+        check(load().gw_simrank_batch(self._h, byref(p), _ptr(a), _ptr(b), nq, R, decay, _ptr(meet), _ptr(scores)),
+              self._h)
+        return scores, meet
+
     def sync(self, stream: int | None = None) -> None:
         check(load().gw_sync(self._h, stream), self._h)
 

@@ -305,6 +305,17 @@ gw_status gw_sync(gw_ctx *ctx, void *stream);
    sum_l meet[l] * 0.8^l / R^2.  R <= 4194240.  Synchronises the stream.     */
 gw_status gw_simrank_meet(gw_ctx *ctx, const uint32_t *d_paths_a, const uint32_t *d_paths_b, uint32_t R,
                           uint32_t L, uint64_t *meet, void *stream);
+/* A batch of SimRank queries (a[q], b[q]) on the resident graph, each as the
+   SimRank app runs one (apps/simrank.cpp:30-84): R walks from each vertex
+   under params->rule = GW_RULE_RESTART (RandomWalkwithRestartwithJoint),
+   replica i starting at hop i*L and keyed on its source vertex, recording
+   L - 1 visits; then the meeting reduction.  Walks are run once per distinct
+   vertex of the batch and shared by its queries (for a[q] == b[q] both sides
+   are the same walks; the app, which files a's walks before b's, would see no
+   walks from b).  meet (host, nq * L, may be NULL) receives each query's
+   first-meeting counts, scores (host, nq) sum_l meet[l] * decay^l / R^2.    */
+gw_status gw_simrank_batch(gw_ctx *ctx, const gw_walk_params *params, const uint32_t *a, const uint32_t *b,
+                           uint32_t nq, uint32_t R, double decay, uint64_t *meet, double *scores);
 
 /* One superstep of the blocked engine that allocates no memory.  This entry
    point has no counterpart in the reference (whose engine allocates host
