@@ -69,7 +69,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-probe", action="store_true", help="skip the random-gather roof probe")
     ap.add_argument("--cpu-sample-sec", type=float, default=15.0)
-    ap.add_argument("--workload", choices=["rawwalk", "msppr", "serve", "ppr1", "ooc", "convert"], default="rawwalk",
+    ap.add_argument("--workload", choices=["rawwalk", "msppr", "serve", "ppr1", "ooc", "convert", "simrank"],
+                    default="rawwalk",
                     help="rawwalk: the headline raw-random-walk step; msppr: batched vs plain multi-source PPR; "
                          "serve: Poisson-arrival PPR serving, continuous batching vs one query per launch")
     ap.add_argument("--rates", default="1000,5000,10000,20000,50000", help="serve: arrival rates (queries/s)")
@@ -798,8 +799,73 @@ def convert_arm(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def simrank_arm(args) -> None:
+    """Batched SimRank (apps/simrank.cpp semantics: R walks of L - 1 hops from
+    each vertex under the restart rule, replica i from hop i*L; first-meeting
+    reduction): queries/s of one gw_simrank_batch call against the reference's
+    simrank app, unchanged, one query per process as it runs."""
+    import numpy as np
+    import torch
+
+    import graphwalker_b200 as gw
+    torch.cuda.set_device(0)
+    R, L, nq = 1000, 11, args.queries
+    kb = blocksize_kb_for(args.scale, args.edge_factor, args.nblocks)
+    G = gw.Graph.rmat(args.scale, args.edge_factor, seed=args.graph_seed, blocksize_kb=kb)
+    rng = np.random.default_rng(13)
+    # the app asserts getblock(a) == getblock(b): pairs inside one block
+    blocks = G.blocks.astype(np.int64)
+    blk = rng.integers(0, G.nblocks, nq)
+    lo, hi = blocks[blk], blocks[blk + 1]
+    a = (lo + rng.integers(0, 1 << 62, nq) % (hi - lo)).astype(np.uint32)
+    b = (lo + rng.integers(0, 1 << 62, nq) % (hi - lo)).astype(np.uint32)
+    for _ in range(max(1, args.warmup)):
+        G.simrank_batch(a, b, R, L, seed=args.walk_seed)
+    times = []
+    with ClockSampler(device_uuid(0)) as clk:
+        for _ in range(max(1, args.steps)):
+            t0 = time.perf_counter()
+            scores, meet = G.simrank_batch(a, b, R, L, seed=args.walk_seed)
+            times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    cpu = None
+    if not args.no_cpu_baseline:
+        rowptr, colidx = G.export_csr()
+        exe = ROOT / "oracle" / "_ref" / "simrank"
+        with tempfile.TemporaryDirectory(prefix="gw_ref_") as td:
+            tmp = Path(td)
+            base, _, _ = write_reference_graph(tmp, args, rowptr, colidx)
+            del rowptr, colidx
+            wall = []
+            for q in range(min(nq, 5)):
+                t0 = time.perf_counter()
+                r = subprocess.run([str(exe), "file", base, "a", str(a[q]), "b", str(b[q]), "R", str(R), "L", str(L),
+                                    "blocksize_kb", str(kb)], cwd=tmp, capture_output=True, text=True, timeout=600)
+                wall.append(time.perf_counter() - t0)
+                if r.returncode != 0:
+                    raise RuntimeError(r.stderr[-500:])
+            cpu = {"value": 1.0 / statistics.median(wall), "unit": "queries/s", "cores": host_cores(),
+                   "kind": "reference",
+                   "sample": f"apps/simrank.cpp unchanged, compiled -O3 from source with native rand_r, one process "
+                             f"per query as the app runs, {len(wall)} queries of the same batch "
+                             f"(median {statistics.median(wall) * 1e3:.1f} ms each, graph files in the page cache)"}
+    line = {"metric": "queries/s", "value": nq / t, "unit": "queries/s", "workload": "simrank", "n_gpus": 1,
+            "steps": max(1, args.steps), "warmup": max(1, args.warmup), "ms_per_step": t * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": f"batched SimRank, R-MAT scale {args.scale} ef {args.edge_factor}, {nq} pairs "
+                                   f"inside one block each, R={R} walks per vertex, L={L}, decay 0.8",
+                       "api": "gw_simrank_batch (host arrays in, scores out)"},
+            "mean_score": float(np.mean(scores)), "pairs_meeting": int((meet.sum(1) > 0).sum()),
+            "cpu_baseline": cpu, "clocks": clk.summary()}
+    G.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.workload == "simrank" and args.impl != "reference":
+        simrank_arm(args)
+        return
     if args.workload == "convert" and args.impl != "reference":
         convert_arm(args)
         return

@@ -556,9 +556,6 @@ gw_status gw_simrank_batch(gw_ctx* ctx, const gw_walk_params* params, const uint
     if (v >= ctx->nv) return ctx->fail(GW_E_INVALID, "SimRank vertex %u >= nvertices", v);
   const uint64_t n = (uint64_t)verts.size() * R;
   if ((uint64_t)(R - 1) * L >= (1ull << 32)) return ctx->fail(GW_E_INVALID, "R * L exceeds the 32-bit hop field");
-  std::vector<gw_walk_rec> recs(n);
-  for (size_t k = 0; k < verts.size(); ++k)
-    for (uint32_t i = 0; i < R; ++i) recs[k * R + i] = gw_walk_rec{verts[k], verts[k], verts[k], i * L};
   std::vector<unsigned long long> rows(2 * (size_t)nq);
   auto row_of = [&](uint32_t v) {
     return (unsigned long long)(std::lower_bound(verts.begin(), verts.end(), v) - verts.begin()) * R * L;
@@ -572,10 +569,12 @@ gw_status gw_simrank_batch(gw_ctx* ctx, const gw_walk_params* params, const uint
   GW_CUDA(ctx, ctx->d_walks.ensure(n * sizeof(gw_walk_rec)), "walk alloc");
   GW_CUDA(ctx, ctx->d_paths.ensure(n * L * 4), "paths alloc");
   GW_CUDA(ctx, ctx->d_plen.ensure(n * 4), "plen alloc");
-  GW_CUDA(ctx, ctx->d_sr_rows.ensure(rows.size() * 8), "rows alloc");
+  GW_CUDA(ctx, ctx->d_sr_rows.ensure(rows.size() * 8 + verts.size() * 4), "rows alloc");
+  uint32_t* d_verts = reinterpret_cast<uint32_t*>(ctx->d_sr_rows.as<char>() + rows.size() * 8);
   GW_CUDA(ctx, ctx->d_meet.ensure((size_t)nq * L * 8), "meet alloc");
-  GW_CUDA(ctx, cudaMemcpyAsync(ctx->d_walks.p, recs.data(), n * sizeof(gw_walk_rec), cudaMemcpyHostToDevice, st),
-          "walk upload");
+  GW_CUDA(ctx, cudaMemcpyAsync(d_verts, verts.data(), verts.size() * 4, cudaMemcpyHostToDevice, st), "vertex upload");
+  GW_CUDA(ctx, gw::launch_simrank_walks(d_verts, (uint32_t)verts.size(), R, L, ctx->d_walks.as<gw_walk_rec>(), st),
+          "simrank placement");
   GW_CUDA(ctx, cudaMemcpyAsync(ctx->d_sr_rows.p, rows.data(), rows.size() * 8, cudaMemcpyHostToDevice, st),
           "rows upload");
   GW_CUDA(ctx, cudaMemsetAsync(ctx->d_paths.p, 0xff, n * L * 4, st), "paths clear");

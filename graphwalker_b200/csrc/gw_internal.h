@@ -55,6 +55,9 @@ cudaError_t launch_pack_words(const gw_walk_rec* walks, uint64_t n, const uint32
 // (rows NULL: one query at offset 0 of both) (gw_simrank.cu).
 cudaError_t launch_simrank_meet(const uint32_t* a, const uint32_t* b, const unsigned long long* rows, uint32_t nq,
                                 uint32_t R, uint32_t L, unsigned long long* meet, cudaStream_t stream);
+// Walk records of SimRank's placement: walk k * R + i = replica i of verts[k].
+cudaError_t launch_simrank_walks(const uint32_t* verts, uint32_t nverts, uint32_t R, uint32_t L, gw_walk_rec* out,
+                                 cudaStream_t stream);
 // erec[e] = (packed record of colidx[e], colidx[e]) for e < ne (gw_walk.cu).
 cudaError_t launch_build_erec(const uint32_t* colidx, const unsigned long long* vrec, uint64_t ne, uint32_t nv,
                               ulonglong2* erec, cudaStream_t stream);

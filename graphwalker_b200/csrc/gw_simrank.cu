@@ -70,7 +70,29 @@ __global__ void __launch_bounds__(kSrThreads)
   }
 }
 
+// The app's placement (simrank.cpp:30-57): replica i of vertex v starts at v
+// with hop i*L, keyed on v; walk k * R + i is replica i of verts[k].
+__global__ void simrank_walks_kernel(const uint32_t* __restrict__ verts, uint64_t n, uint32_t R, uint32_t L,
+                                     gw_walk_rec* __restrict__ out) {
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < n; w += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = __ldg(verts + w / R), i = (uint32_t)(w % R);
+    reinterpret_cast<uint4*>(out)[w] = make_uint4(v, v, v, i * L);
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_simrank_walks(const uint32_t* verts, uint32_t nverts, uint32_t R, uint32_t L, gw_walk_rec* out,
+                                 cudaStream_t stream) {
+  const uint64_t n = (uint64_t)nverts * R;
+  if (n == 0) return cudaSuccess;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const uint64_t need = (n + 255) / 256, cap = (uint64_t)sms * 16;
+  simrank_walks_kernel<<<(unsigned)(need < cap ? need : cap), 256, 0, stream>>>(verts, n, R, L, out);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_simrank_meet(const uint32_t* a, const uint32_t* b, const unsigned long long* rows, uint32_t nq,
                                 uint32_t R, uint32_t L, unsigned long long* meet, cudaStream_t stream) {
