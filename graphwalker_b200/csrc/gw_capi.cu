@@ -186,11 +186,19 @@ gw_status make_walk_args(gw_ctx* ctx, const gw_walk_params* p, WalkArgs* a) {
   return GW_OK;
 }
 
+cudaError_t enqueue_status_read(gw_ctx* ctx, cudaStream_t stream) {
+  cudaError_t e = cudaMemcpyAsync(ctx->h_status.p, ctx->d_status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_status.p, 0, sizeof(uint32_t), stream);
+  return e;
+}
+
 gw_status take_status(gw_ctx* ctx, cudaStream_t stream) {
-  GW_CUDA(ctx, cudaMemcpyAsync(ctx->h_status.p, ctx->d_status.p, sizeof(uint32_t),
-                               cudaMemcpyDeviceToHost, stream), "status read");
-  GW_CUDA(ctx, cudaMemsetAsync(ctx->d_status.p, 0, sizeof(uint32_t), stream), "status clear");
+  GW_CUDA(ctx, enqueue_status_read(ctx, stream), "status read");
   GW_CUDA(ctx, cudaStreamSynchronize(stream), "synchronize");
+  return read_status(ctx);
+}
+
+gw_status read_status(gw_ctx* ctx) {
   const uint32_t st = *ctx->h_status.as<uint32_t>();
   if (st & kStBounds) return ctx->fail(GW_E_BOUNDS, "a walk reached a vertex id >= %u", ctx->nv);
   if (st & kStOverflow) return ctx->fail(GW_E_OVERFLOW, "a walk made more visits than path_stride");

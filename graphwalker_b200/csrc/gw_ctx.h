@@ -155,6 +155,10 @@ gw_status thread_error(gw_status code, const std::string& msg);
 gw_status make_walk_args(gw_ctx* ctx, const gw_walk_params* p, WalkArgs* a);
 // Reads and clears the device status word (synchronises ctx->stream).
 gw_status take_status(gw_ctx* ctx, cudaStream_t stream);
+// The same in two halves: enqueue the read and clear on a stream, then, after
+// the caller has synchronised it, interpret the word.
+cudaError_t enqueue_status_read(gw_ctx* ctx, cudaStream_t stream);
+gw_status read_status(gw_ctx* ctx);
 // GraphWalker's block loop on the device (gw_engine.cu).
 gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p);
 }  // namespace gw

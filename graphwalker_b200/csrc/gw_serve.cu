@@ -16,6 +16,7 @@
 // budget and stream, not on what it was mixed with.  A query whose table fills
 // up is restarted with a table four times larger (same draws, same result).
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -35,6 +36,10 @@ uint64_t now_ns() {
              std::chrono::steady_clock::now().time_since_epoch())
       .count();
 }
+
+// Arrivals closer than this are waited for by spinning (yielding) rather
+// than by a timed sleep.
+constexpr uint64_t kSpinNs = 300000;
 
 uint64_t pow2_at_least(uint64_t x) {
   uint64_t p = 1;
@@ -104,6 +109,9 @@ struct gw_server {
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   bool stop = false;
+  // earliest arrival the scheduler may be spinning for; a submission of an
+  // earlier query lowers it so the spin ends at once
+  std::atomic<uint64_t> next_due{~0ull};
   uint64_t next_ticket = 1;
   std::deque<uint64_t> pending;              // submitted, not admitted (FIFO)
   std::vector<uint64_t> active;              // admitted, not complete
@@ -264,12 +272,13 @@ bool superstep(gw_server* srv) {
   if (e == cudaSuccess && nfin) e = gw::launch_topk(qv, 0, nfin, k, d.ids, d.counts, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(h.full, d.full, n * 4, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(h.ids, d.ids, (size_t)n * k * 4 * 2, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = gw::enqueue_status_read(ctx, st);  // one synchronisation for results and status
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     srv->fatal = ctx->cuda_fail(e, "serve superstep");
     return false;
   }
-  const gw_status status = gw::take_status(ctx, st);
+  const gw_status status = gw::read_status(ctx);
   const uint64_t t = now_ns();
   std::lock_guard<std::mutex> lock(srv->mu);
   srv->stats.supersteps++;
@@ -329,7 +338,15 @@ void serve_loop(gw_server* srv) {
           const uint64_t due = srv->queries[srv->pending.front()].arrival_ns;
           const uint64_t t = now_ns();
           if (due <= t) break;
-          srv->cv_work.wait_for(lock, std::chrono::nanoseconds(due - t));
+          if (due - t > kSpinNs) {  // sleep until shortly before the arrival
+            srv->cv_work.wait_for(lock, std::chrono::nanoseconds(due - t - kSpinNs));
+            continue;
+          }
+          // the last stretch is spun: a timed sleep wakes tens of microseconds late
+          srv->next_due.store(due);
+          lock.unlock();
+          while (now_ns() < srv->next_due.load(std::memory_order_relaxed)) std::this_thread::yield();
+          lock.lock();
           continue;
         }
         srv->cv_work.wait(lock);
@@ -410,6 +427,9 @@ gw_status gw_serve_submit(gw_server* srv, uint32_t source, uint32_t budget, uint
   while (pos != srv->pending.begin() && srv->queries[*std::prev(pos)].arrival_ns > srv->queries[t].arrival_ns) --pos;
   srv->pending.insert(pos, t);
   srv->stats.submitted++;
+  uint64_t due = srv->next_due.load();
+  while (srv->queries[t].arrival_ns < due && !srv->next_due.compare_exchange_weak(due, srv->queries[t].arrival_ns)) {
+  }
   *ticket = t;
   srv->cv_work.notify_one();
   return GW_OK;
