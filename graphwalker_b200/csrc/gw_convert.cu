@@ -16,10 +16,13 @@
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cub/cub.cuh>
@@ -32,7 +35,7 @@ namespace gw {
 namespace {
 
 constexpr uint32_t kMaxLine = 1023;          // fgets(s, 1024, f) reads at most 1023 bytes
-constexpr size_t kChunkBytes = 128ull << 20;  // text per device round (GW_CONVERT_CHUNK_BYTES overrides)
+constexpr size_t kChunkBytes = 64ull << 20;  // text per device round (GW_CONVERT_CHUNK_BYTES overrides)
 constexpr unsigned long long kNoLine = ~0ull;
 
 struct LineStartAt {
@@ -159,11 +162,54 @@ int remove_tree(const std::string& path) {  // rm_dir (conversions.hpp:42-81)
   return rmdir(path.c_str());
 }
 
+// Host threads for file reads and writes: copies between the page cache and
+// user memory run at a few GB/s per thread.
+unsigned io_threads() {
+  const unsigned h = std::thread::hardware_concurrency();
+  return h == 0 ? 1u : std::min(h, 8u);
+}
+
+// pread/pwrite of [off, off + bytes) in slices on io_threads() threads; false
+// on an I/O error.  `done` (pread only) receives the bytes transferred.
+bool parallel_io(int fd, char* p, size_t bytes, uint64_t off, bool write, size_t* done) {
+  const unsigned nt = bytes < (8u << 20) ? 1u : io_threads();
+  std::vector<size_t> got(nt, 0);
+  std::vector<char> bad(nt, 0);
+  auto part = [&](unsigned t) {
+    const size_t lo = bytes * t / nt, hi = bytes * (t + 1) / nt;
+    size_t k = lo;
+    while (k < hi) {
+      const ssize_t r = write ? pwrite(fd, p + k, hi - k, (off_t)(off + k)) : pread(fd, p + k, hi - k, (off_t)(off + k));
+      if (r < 0) {
+        bad[t] = 1;
+        break;
+      }
+      if (r == 0) break;  // end of file
+      k += (size_t)r;
+    }
+    got[t] = k - lo;
+  };
+  if (nt == 1) {
+    part(0);
+  } else {
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t) th.emplace_back(part, t);
+    for (auto& x : th) x.join();
+  }
+  size_t total = 0;
+  for (unsigned t = 0; t < nt; ++t) {
+    if (bad[t]) return false;
+    total += got[t];
+  }
+  if (done) *done = total;
+  return total == bytes || !write;
+}
+
 bool write_all(const std::string& path, const void* p, size_t bytes) {
-  FILE* f = fopen(path.c_str(), "wb");
-  if (!f) return false;
-  const bool ok = bytes == 0 || fwrite(p, 1, bytes, f) == bytes;
-  return fclose(f) == 0 && ok;
+  const int fd = open(path.c_str(), O_WRONLY | O_CREAT | O_TRUNC, 0644);
+  if (fd < 0) return false;
+  const bool ok = bytes == 0 || parallel_io(fd, const_cast<char*>(static_cast<const char*>(p)), bytes, 0, true, nullptr);
+  return close(fd) == 0 && ok;
 }
 
 // Device and pinned buffers of one conversion.
@@ -246,24 +292,21 @@ gw_status convert(const char* path, uint64_t blocksize_kb, int32_t device, gw_co
   int cur = 0;
   bool eof = false;
   double ms_read = 0;
+  uint64_t file_pos = 0;
   // reads the next piece of the file behind `carry` bytes of buffer b
   auto fill = [&](int b, size_t head, size_t* got) -> bool {
     const auto t0 = std::chrono::steady_clock::now();
-    char* p = c.host[b].as<char>() + head;
-    size_t want = chunk - head, have = 0;
-    while (have < want) {
-      const ssize_t r = read(fd, p + have, want - have);
-      if (r < 0) return false;
-      if (r == 0) {
-        eof = true;
-        break;
-      }
-      have += (size_t)r;
-    }
+    const size_t want = (size_t)std::min<uint64_t>(chunk - head, s.bytes - file_pos);
+    size_t have = 0;
+    if (want && (!parallel_io(fd, c.host[b].as<char>() + head, want, file_pos, false, &have) || have != want))
+      return false;  // an I/O error, or the file shrank while it was read
+    file_pos += have;
+    if (file_pos >= s.bytes) eof = true;
     *got = head + have;
     ms_read += ms_since(t0);
     return true;
   };
+  uint64_t edge_cap = 0;  // edges the device buffer holds
   size_t avail = 0;
   if (!fill(cur, 0, &avail)) return thread_error(GW_E_IO, std::string("read error on ") + path);
   gw_status status = GW_OK;
@@ -290,7 +333,11 @@ gw_status convert(const char* path, uint64_t blocksize_kb, int32_t device, gw_co
     GW_CV(cudaStreamSynchronize(c.st), "sync");
     GW_CV(c.tmp_edges.ensure(nlines * 8 + 8), "edge buffer");
     GW_CV(c.keep.ensure(nlines + 8), "flags");
-    GW_CV(grow(&c.edges, (ne + nlines) * 8 + 8, ne * 8, c.st), "edge buffer");
+    if (ne + nlines > edge_cap) {  // grow by half again, or to the file's edge estimate from this round
+      const uint64_t estimate = (uint64_t)((double)s.bytes / (double)std::max<size_t>(n, 1) * (double)nlines * 1.05);
+      edge_cap = std::max<uint64_t>({ne + nlines, edge_cap + edge_cap / 2, estimate});
+      GW_CV(grow(&c.edges, edge_cap * 8 + 8, ne * 8, c.st), "edge buffer");
+    }
     const unsigned long long none = kNoLine;
     GW_CV(cudaMemcpyAsync(d_bad, &none, 8, cudaMemcpyHostToDevice, c.st), "bad line");
     if (nlines) {
@@ -370,10 +417,8 @@ gw_status convert(const char* path, uint64_t blocksize_kb, int32_t device, gw_co
   GW_CV(launch_rowptr_from_sorted(keys, ne, (uint32_t)nv, c.rowptr.as<unsigned long long>(), c.colidx.as<uint32_t>(),
                                   c.st),
         "row pointer");
-  std::vector<uint64_t> rowptr(nv + 1);
-  std::vector<uint32_t> colidx(ne);
-  GW_CV(cudaMemcpyAsync(rowptr.data(), c.rowptr.p, (nv + 1) * 8, cudaMemcpyDeviceToHost, c.st), "row pointer copy");
-  if (ne) GW_CV(cudaMemcpyAsync(colidx.data(), c.colidx.p, ne * 4, cudaMemcpyDeviceToHost, c.st), "column copy");
+  std::unique_ptr<uint64_t[]> rowptr(new uint64_t[nv + 1]);  // filled by the copy: no zeroing
+  GW_CV(cudaMemcpyAsync(rowptr.get(), c.rowptr.p, (nv + 1) * 8, cudaMemcpyDeviceToHost, c.st), "row pointer copy");
   GW_CV(cudaStreamSynchronize(c.st), "sync");
   s.ms_device = ms_since(t_start) - s.ms_read;
 
@@ -383,14 +428,34 @@ gw_status convert(const char* path, uint64_t blocksize_kb, int32_t device, gw_co
   remove_tree(dir);
   mkdir(dir.c_str(), 0777);
   mkdir((dir + "/graphinfo").c_str(), 0777);
-  bool ok = write_all(dir + "/graphinfo/file_0.beg_pos", rowptr.data(), rowptr.size() * 8) &&
-            write_all(dir + "/graphinfo/file_0.csr", colidx.data(), colidx.size() * 4);
+  bool ok = write_all(dir + "/graphinfo/file_0.beg_pos", rowptr.get(), (nv + 1) * 8);
+  {  // the column array goes to the file through the two pinned buffers: copy slice k+1 while slice k is written
+    const int cf = open((dir + "/graphinfo/file_0.csr").c_str(), O_WRONLY | O_CREAT | O_TRUNC, 0644);
+    ok = ok && cf >= 0;
+    const size_t slice = chunk / 4 * 4;
+    cudaEvent_t copied[2];
+    for (auto& ev : copied) GW_CV(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+    auto issue = [&](uint64_t off, int b) {
+      const size_t m = (size_t)std::min<uint64_t>(slice, ne * 4 - off);
+      cudaMemcpyAsync(c.host[b].p, c.colidx.as<char>() + off, m, cudaMemcpyDeviceToHost, c.st);
+      cudaEventRecord(copied[b], c.st);
+    };
+    if (ok && ne) issue(0, 0);
+    for (uint64_t off = 0, b = 0; ok && off < ne * 4; off += slice, b ^= 1) {
+      if (off + slice < ne * 4) issue(off + slice, (int)(b ^ 1));
+      ok = cudaEventSynchronize(copied[b]) == cudaSuccess &&
+           parallel_io(cf, c.host[b].as<char>(), (size_t)std::min<uint64_t>(slice, ne * 4 - off), off, true, nullptr);
+    }
+    cudaStreamSynchronize(c.st);  // no copy may be left writing a pinned buffer
+    for (auto& ev : copied) cudaEventDestroy(ev);
+    if (cf >= 0 && close(cf) != 0) ok = false;
+  }
   const std::string nvs = std::to_string(nv) + "\n";
   ok = ok && write_all(dir + "/filesize_1024GB.filerange", ("0\n" + nvs).data(), 2 + nvs.size()) &&
        write_all(dir + "/N.nvertices", nvs.data(), nvs.size());
   if (ok && blocksize_kb) {
     std::vector<uint32_t> blocks(nv + 2);
-    const uint32_t nb = gw_compute_blocks(rowptr.data(), (uint32_t)nv, blocksize_kb, blocks.data(),
+    const uint32_t nb = gw_compute_blocks(rowptr.get(), (uint32_t)nv, blocksize_kb, blocks.data(),
                                           (uint32_t)blocks.size());
     std::string txt;
     for (uint32_t i = 0; i < nb; ++i) txt += std::to_string(blocks[i]) + "\n";
