@@ -198,8 +198,9 @@ gw_status take_status(gw_ctx* ctx, cudaStream_t stream) {
   return read_status(ctx);
 }
 
-gw_status read_status(gw_ctx* ctx) {
-  const uint32_t st = *ctx->h_status.as<uint32_t>();
+gw_status read_status(gw_ctx* ctx) { return status_of(ctx, *ctx->h_status.as<uint32_t>()); }
+
+gw_status status_of(gw_ctx* ctx, uint32_t st) {
   if (st & kStBounds) return ctx->fail(GW_E_BOUNDS, "a walk reached a vertex id >= %u", ctx->nv);
   if (st & kStOverflow) return ctx->fail(GW_E_OVERFLOW, "a walk made more visits than path_stride");
   if (st & kStHops) return ctx->fail(GW_E_OVERFLOW, "an uncapped walk exceeded max_hops");

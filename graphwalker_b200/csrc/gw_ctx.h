@@ -159,6 +159,8 @@ gw_status take_status(gw_ctx* ctx, cudaStream_t stream);
 // the caller has synchronised it, interpret the word.
 cudaError_t enqueue_status_read(gw_ctx* ctx, cudaStream_t stream);
 gw_status read_status(gw_ctx* ctx);
+// The error a status word's bits stand for (GW_OK for none).
+gw_status status_of(gw_ctx* ctx, uint32_t bits);
 // GraphWalker's block loop on the device (gw_engine.cu).
 gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p);
 }  // namespace gw

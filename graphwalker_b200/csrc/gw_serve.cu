@@ -129,14 +129,17 @@ struct gw_server {
 namespace {
 
 // Staging layout for up to n queries in one superstep: the launch's chunk
-// cursor, then the 8-byte and 4-byte per-query fields, then the top-k output.
+// cursor; the per-query inputs (copied up); then the results, one contiguous
+// range copied back: the launch's status word, the table-full flags and the
+// top-k lists.  The status word and the flags are also copied up, as zeros.
 struct Stage {
   unsigned long long *cursor, *prefix, *id_base, *toff;
-  uint32_t *sources, *tmask, *full, *stream, *ids, *counts;
+  uint32_t *sources, *tmask, *stream, *status, *full, *ids, *counts;
 };
 
 size_t stage_bytes(uint32_t n, uint32_t k) {
-  return 8 + (size_t)(n + 1) * 8 + 2 * (size_t)n * 8 + 4 * (size_t)n * 4 + 2 * (size_t)n * k * 4;
+  return 8 + (size_t)(n + 1) * 8 + 2 * (size_t)n * 8 + 3 * (size_t)n * 4 + 4 + (size_t)n * 4 +
+         2 * (size_t)n * k * 4;
 }
 
 Stage carve(void* base, uint32_t n, uint32_t k) {
@@ -154,9 +157,11 @@ Stage carve(void* base, uint32_t n, uint32_t k) {
   p += (size_t)n * 4;
   s.tmask = reinterpret_cast<uint32_t*>(p);
   p += (size_t)n * 4;
-  s.full = reinterpret_cast<uint32_t*>(p);
-  p += (size_t)n * 4;
   s.stream = reinterpret_cast<uint32_t*>(p);
+  p += (size_t)n * 4;
+  s.status = reinterpret_cast<uint32_t*>(p);
+  p += 4;
+  s.full = reinterpret_cast<uint32_t*>(p);
   p += (size_t)n * 4;
   s.ids = reinterpret_cast<uint32_t*>(p);
   p += (size_t)n * k * 4;
@@ -261,24 +266,25 @@ bool superstep(gw_server* srv) {
     acc += take[i];
   }
   h.prefix[n] = acc;
-  const size_t head = stage_bytes(n, k) - 8 - 2 * (size_t)n * k * 4;
+  h.status[0] = 0;
+  const size_t head = stage_bytes(n, k) - 8 - 2 * (size_t)n * k * 4;  // prefix .. full
   cudaError_t e = cudaMemcpyAsync(d.prefix, h.prefix, head, cudaMemcpyHostToDevice, st);
   gw::QueryView qv = make_view(d, srv->tables.as<unsigned long long>(), n);
   qv.chunk = ctx->ppr_chunk;
   if (e == cudaSuccess)
-    e = gw::launch_walk_queries((int)srv->params.rule, qv, 0, acc, ctx->view(), srv->args,
-                                ctx->d_status.as<uint32_t>(), ctx->ppr_threads_per_sm, st);
+    e = gw::launch_walk_queries((int)srv->params.rule, qv, 0, acc, ctx->view(), srv->args, d.status,
+                                ctx->ppr_threads_per_sm, st);
   // queries whose last walks are in this superstep get their top-k now
   if (e == cudaSuccess && nfin) e = gw::launch_topk(qv, 0, nfin, k, d.ids, d.counts, st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(h.full, d.full, n * 4, cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(h.ids, d.ids, (size_t)n * k * 4 * 2, cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = gw::enqueue_status_read(ctx, st);  // one synchronisation for results and status
+  // status, flags and lists come back in one copy, then one synchronisation
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h.status, d.status, 4 + (size_t)n * 4 + (size_t)n * k * 4 * 2, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     srv->fatal = ctx->cuda_fail(e, "serve superstep");
     return false;
   }
-  const gw_status status = gw::read_status(ctx);
+  const gw_status status = gw::status_of(ctx, h.status[0]);
   const uint64_t t = now_ns();
   std::lock_guard<std::mutex> lock(srv->mu);
   srv->stats.supersteps++;
