@@ -446,7 +446,7 @@ gw_status gw_close(gw_ctx* ctx) {
                        &ctx->d_scan_temp, &ctx->d_out_ptr, &ctx->d_out_base, &ctx->d_q_sources,
                        &ctx->d_q_prefix, &ctx->d_q_idbase, &ctx->d_q_toff, &ctx->d_q_tmask, &ctx->d_q_tables,
                        &ctx->d_q_full, &ctx->d_q_ids, &ctx->d_q_counts, &ctx->d_q_visits,
-                       &ctx->d_q_cursor})
+                       &ctx->d_q_cursor, &ctx->d_q_segs, &ctx->d_q_cand})
     b->release();
   for (gw_devbuf& b : ctx->pools) b.release();
   ctx->h_rowptr.release();

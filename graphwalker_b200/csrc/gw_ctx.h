@@ -103,7 +103,7 @@ struct gw_ctx {
 
   // multi-source PPR queries
   gw_devbuf d_q_sources, d_q_prefix, d_q_idbase, d_q_toff, d_q_tmask, d_q_tables, d_q_full, d_q_ids,
-      d_q_counts, d_q_visits, d_q_cursor;
+      d_q_counts, d_q_visits, d_q_cursor, d_q_segs, d_q_cand;
   int ppr_threads_per_sm = 0;  // autotuned launch shape (0 = full occupancy)
   uint32_t ppr_chunk = 0;      // autotuned walks per cursor grab (0 = default)
 

@@ -15,11 +15,12 @@
 // of consecutive batch positions from a global cursor, so the walks in flight
 // belong to a narrow window of queries whose tables stay in L2.
 //
-// Top-k: one CTA per query scans its table and keeps a candidate buffer of
-// keys (count << 32 | ~vertex): whenever the buffer could overflow it is
-// sorted and cut to the best k, and the k-th key becomes the admission
-// threshold.  The result is the exact top k by count, ties broken by the
-// smaller vertex id.
+// Top-k: a CTA scans a table (or a segment of one) and keeps a candidate
+// buffer of keys (count << 32 | ~vertex): whenever the buffer could overflow
+// it is sorted and cut to the best k, and the k-th key becomes the admission
+// threshold.  Large tables are split into segments ranked by separate CTAs,
+// whose lists a second kernel merges.  The result is the exact top k by
+// count, ties broken by the smaller vertex id.
 #include "gw_ppr.h"
 
 namespace gw {
@@ -268,39 +269,34 @@ __device__ void block_sort_desc(unsigned long long* keys, uint32_t n) {
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kTopkThreads)
-    topk_kernel(QueryView qv, uint32_t q_begin, uint32_t k, uint32_t* __restrict__ out_ids,
-                uint32_t* __restrict__ out_counts) {
-  __shared__ unsigned long long cand[kTopkBuffer];
-  __shared__ uint32_t ncand;
-  __shared__ unsigned long long thresh;
-  const uint32_t q = q_begin + blockIdx.x;
-  const unsigned long long* t = qv.tables + qv.table_off[q];
-  const uint32_t cap = qv.table_mask[q] + 1;
+// The best k keys of n (key i = src.key(src.fetch(i)); 0 = no key) into
+// cand[0, k), largest first.  kTopkUnroll values per thread are fetched
+// before any is converted (the loads issue back to back, so a large table is
+// read with that many loads in flight per thread), then filtered one round of
+// blockDim.x keys at a time into the candidate buffer; whenever the buffer
+// could overflow it is sorted and cut to the best k, and the k-th key becomes
+// the admission threshold.
+template <typename Src>
+__device__ void block_best(Src src, uint32_t n, uint32_t k, unsigned long long* cand, uint32_t& ncand,
+                           unsigned long long& thresh) {
   if (threadIdx.x == 0) {
     ncand = 0;
     thresh = 0;
   }
   __syncthreads();
-  // kTopkUnroll slots per thread are loaded together (so a large table is
-  // read with that many loads in flight per thread), then filtered one round
-  // of blockDim.x slots at a time.
-  const uint64_t pol = l2_policy(true, false);
-  for (uint32_t base = 0; base < cap; base += blockDim.x * kTopkUnroll) {
-    unsigned long long e[kTopkUnroll];
+  for (uint32_t base = 0; base < n; base += blockDim.x * kTopkUnroll) {
+    unsigned long long raw[kTopkUnroll];
 #pragma unroll
     for (uint32_t u = 0; u < kTopkUnroll; ++u) {
       const uint32_t i = base + u * blockDim.x + threadIdx.x;
-      e[u] = i < cap ? ld_nc_u64(t + i, pol) : kEmptySlot;
+      raw[u] = i < n ? src.fetch(i) : Src::kNone;
     }
 #pragma unroll
     for (uint32_t u = 0; u < kTopkUnroll; ++u) {
-      if (e[u] != kEmptySlot) {
-        const unsigned long long key = ((e[u] & 0xffffffffull) << 32) | (uint32_t)~(uint32_t)(e[u] >> 32);
-        if (key > thresh) {
-          const uint32_t pos = atomicAdd(&ncand, 1u);
-          cand[pos] = key;  // room for one full round is kept free below
-        }
+      const unsigned long long key = Src::key(raw[u]);
+      if (key > thresh) {
+        const uint32_t pos = atomicAdd(&ncand, 1u);
+        cand[pos] = key;  // room for one full round is kept free below
       }
       __syncthreads();
       if (ncand > kTopkBuffer - blockDim.x) {  // cut to the best k before the next round
@@ -316,11 +312,92 @@ __global__ void __launch_bounds__(kTopkThreads)
   }
   for (uint32_t x = ncand + threadIdx.x; x < kTopkBuffer; x += blockDim.x) cand[x] = 0;
   block_sort_desc(cand, kTopkBuffer);
+}
+
+// Key of a table slot: count << 32 | ~vertex (larger = more visits, then the
+// smaller vertex id); 0 for an empty slot.
+struct SlotKey {
+  static constexpr unsigned long long kNone = kEmptySlot;
+  const unsigned long long* t;
+  uint64_t pol;
+  __device__ unsigned long long fetch(uint32_t i) const { return ld_nc_u64(t + i, pol); }
+  __device__ static unsigned long long key(unsigned long long e) {
+    return e == kEmptySlot ? 0ull : ((e & 0xffffffffull) << 32) | (uint32_t)~(uint32_t)(e >> 32);
+  }
+};
+
+struct CandKey {  // candidate lists hold keys already (0 = none)
+  static constexpr unsigned long long kNone = 0ull;
+  const unsigned long long* c;
+  __device__ unsigned long long fetch(uint32_t i) const { return c[i]; }
+  __device__ static unsigned long long key(unsigned long long v) { return v; }
+};
+
+__device__ void write_topk(const unsigned long long* cand, uint32_t q, uint32_t k, uint32_t* out_ids,
+                           uint32_t* out_counts) {
   for (uint32_t r = threadIdx.x; r < k; r += blockDim.x) {
     const unsigned long long key = cand[r];
     out_ids[(unsigned long long)q * k + r] = key ? ~(uint32_t)key : 0xffffffffu;
     out_counts[(unsigned long long)q * k + r] = (uint32_t)(key >> 32);
   }
+}
+
+// One CTA per query over its whole table.
+__global__ void __launch_bounds__(kTopkThreads)
+    topk_kernel(QueryView qv, uint32_t q_begin, uint32_t k, uint32_t* __restrict__ out_ids,
+                uint32_t* __restrict__ out_counts) {
+  __shared__ unsigned long long cand[kTopkBuffer];
+  __shared__ uint32_t ncand;
+  __shared__ unsigned long long thresh;
+  const uint32_t q = q_begin + blockIdx.x;
+  block_best(SlotKey{qv.tables + qv.table_off[q], l2_policy(true, false)}, qv.table_mask[q] + 1, k, cand, ncand,
+             thresh);
+  write_topk(cand, q, k, out_ids, out_counts);
+}
+
+// One CTA per table segment of seg_slots slots: a query with one segment
+// gets its list here; the others leave their segments' best k keys in
+// seg_cand for topk_merge_kernel.
+__global__ void __launch_bounds__(kTopkThreads)
+    topk_segment_kernel(QueryView qv, uint32_t q_begin, uint32_t q_count, uint32_t k, uint32_t seg_slots,
+                        const unsigned long long* __restrict__ seg_first, unsigned long long* __restrict__ seg_cand,
+                        uint32_t* __restrict__ out_ids, uint32_t* __restrict__ out_counts) {
+  __shared__ unsigned long long cand[kTopkBuffer];
+  __shared__ uint32_t ncand;
+  __shared__ unsigned long long thresh;
+  const unsigned long long g = seg_first[q_begin] + blockIdx.x;
+  uint32_t lo = q_begin, hi = q_begin + q_count - 1;  // the query holding segment g
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (seg_first[mid] <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  const uint32_t q = lo;
+  const unsigned long long nseg = seg_first[q + 1] - seg_first[q];
+  const uint32_t cap = qv.table_mask[q] + 1;
+  const uint32_t first = (uint32_t)(g - seg_first[q]) * seg_slots;
+  const uint32_t n = cap - first < seg_slots ? cap - first : seg_slots;
+  block_best(SlotKey{qv.tables + qv.table_off[q] + first, l2_policy(true, false)}, n, k, cand, ncand, thresh);
+  if (nseg == 1) {
+    write_topk(cand, q, k, out_ids, out_counts);
+  } else {
+    for (uint32_t r = threadIdx.x; r < k; r += blockDim.x) seg_cand[g * k + r] = cand[r];
+  }
+}
+
+// One CTA per query with several segments: the best k of its segments' lists.
+__global__ void __launch_bounds__(kTopkThreads)
+    topk_merge_kernel(uint32_t q_begin, uint32_t k, const unsigned long long* __restrict__ seg_first,
+                      const unsigned long long* __restrict__ seg_cand, uint32_t* __restrict__ out_ids,
+                      uint32_t* __restrict__ out_counts) {
+  __shared__ unsigned long long cand[kTopkBuffer];
+  __shared__ uint32_t ncand;
+  __shared__ unsigned long long thresh;
+  const uint32_t q = q_begin + blockIdx.x;
+  const unsigned long long s0 = seg_first[q], nseg = seg_first[q + 1] - s0;
+  if (nseg < 2) return;
+  block_best(CandKey{seg_cand + s0 * k}, (uint32_t)(nseg * k), k, cand, ncand, thresh);
+  write_topk(cand, q, k, out_ids, out_counts);
 }
 
 __global__ void clear_tables_kernel(ulonglong2* __restrict__ t, unsigned long long n2) {
@@ -383,6 +460,40 @@ cudaError_t launch_clear_tables(unsigned long long* tables, unsigned long long n
   clear_tables_kernel<<<(unsigned)(need < full ? need : full), 256, 0, stream>>>(
       reinterpret_cast<ulonglong2*>(tables), n2);
   return cudaGetLastError();
+}
+
+uint32_t topk_segment_slots(uint32_t nq) {
+  uint64_t s = kTopkSegment;
+  while (s < (1ull << 30) && s / kTopkSegment * 64 < nq) s <<= 1;  // 64 queries per doubling
+  return (uint32_t)s;
+}
+
+void topk_segment_prefix(const uint32_t* table_mask, uint32_t nq, uint32_t seg_slots, unsigned long long* seg_first) {
+  seg_first[0] = 0;
+  for (uint32_t q = 0; q < nq; ++q)
+    seg_first[q + 1] = seg_first[q] + ((unsigned long long)table_mask[q] + seg_slots) / seg_slots;
+}
+
+cudaError_t launch_topk_segmented(const QueryView& qv, uint32_t q_begin, uint32_t q_count, uint32_t k,
+                                  uint32_t* out_ids, uint32_t* out_counts, const unsigned long long* d_seg_first,
+                                  const unsigned long long* h_seg_first, uint32_t seg_slots,
+                                  unsigned long long* d_seg_cand, cudaStream_t stream) {
+  if (q_count == 0) return cudaSuccess;
+  if (k == 0 || k > kTopkMaxK) return cudaErrorInvalidValue;
+  const unsigned long long nseg = h_seg_first[q_begin + q_count] - h_seg_first[q_begin];
+  if (nseg == 0 || nseg > 0x7fffffffull) return cudaErrorInvalidValue;
+  if (nseg == q_count) {  // no table is split: one CTA per query
+    topk_kernel<<<q_count, kTopkThreads, 0, stream>>>(qv, q_begin, k, out_ids, out_counts);
+    return cudaGetLastError();
+  }
+  topk_segment_kernel<<<(unsigned)nseg, kTopkThreads, 0, stream>>>(qv, q_begin, q_count, k, seg_slots, d_seg_first,
+                                                                    d_seg_cand, out_ids, out_counts);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && nseg > q_count) {  // some query has several segments
+    topk_merge_kernel<<<q_count, kTopkThreads, 0, stream>>>(q_begin, k, d_seg_first, d_seg_cand, out_ids, out_counts);
+    e = cudaGetLastError();
+  }
+  return e;
 }
 
 cudaError_t launch_topk(const QueryView& qv, uint32_t q_begin, uint32_t q_count, uint32_t k, uint32_t* out_ids,

@@ -10,6 +10,7 @@ constexpr int kTopkThreads = 512;
 constexpr uint32_t kTopkBuffer = 1024;  // candidate keys per CTA
 constexpr uint32_t kTopkMaxK = kTopkBuffer - kTopkThreads;
 constexpr uint32_t kTopkUnroll = 8;     // table slots a top-k thread loads at once
+constexpr uint32_t kTopkSegment = 16384;  // fewest table slots one top-k CTA ranks (segmented top-k)
 
 // Walks a warp takes from the batch cursor at a time, by default: small
 // enough that the walks in flight stay inside a narrow window of the batch
@@ -39,7 +40,21 @@ cudaError_t launch_walk_queries(int rule, const QueryView& qv, unsigned long lon
                                 uint32_t* status, int threads_per_sm, cudaStream_t stream);
 // Sets slots [0, n) of a table area to empty.
 cudaError_t launch_clear_tables(unsigned long long* tables, unsigned long long n, cudaStream_t stream);
-// Top-k of queries [q_begin, q_begin + q_count) into out[q * k + r].
+// Table slots per top-k segment for a set of nq queries: kTopkSegment for a
+// few queries (one large table is split over many CTAs), growing with nq so
+// that a large batch, which fills the GPU with whole tables, is not split
+// into small segments that each pay for their own sorts.
+uint32_t topk_segment_slots(uint32_t nq);
+// seg_first[q + 1] = seg_first[q] + segments of query q's table (host).
+void topk_segment_prefix(const uint32_t* table_mask, uint32_t nq, uint32_t seg_slots, unsigned long long* seg_first);
+// Top-k of queries [q_begin, q_begin + q_count) into out[q * k + r], one CTA
+// per kTopkSegment slots of table: seg_first (nq + 1, on the device and the
+// host) from topk_segment_prefix, seg_cand k keys of scratch per segment.
+cudaError_t launch_topk_segmented(const QueryView& qv, uint32_t q_begin, uint32_t q_count, uint32_t k,
+                                  uint32_t* out_ids, uint32_t* out_counts, const unsigned long long* d_seg_first,
+                                  const unsigned long long* h_seg_first, uint32_t seg_slots,
+                                  unsigned long long* d_seg_cand, cudaStream_t stream);
+// Top-k of queries [q_begin, q_begin + q_count) into out[q * k + r], one CTA per query.
 cudaError_t launch_topk(const QueryView& qv, uint32_t q_begin, uint32_t q_count, uint32_t k, uint32_t* out_ids,
                         uint32_t* out_counts, cudaStream_t stream);
 

@@ -28,17 +28,21 @@ struct QuerySet {
   std::vector<uint32_t> sources, qmap;  // qmap: index in the caller's query list
   std::vector<unsigned long long> prefix, id_base, toff;
   std::vector<uint32_t> tmask;
+  std::vector<unsigned long long> seg_first;  // top-k segments per query (prefix)
+  uint32_t seg_slots = gw::kTopkSegment;
   uint64_t walks = 0, slots = 0;
-  gw_devbuf own[10];
-  gw_devbuf *d_sources, *d_prefix, *d_id_base, *d_toff, *d_tmask, *d_tables, *d_full, *d_ids, *d_cnt, *d_cursor;
+  gw_devbuf own[12];
+  gw_devbuf *d_sources, *d_prefix, *d_id_base, *d_toff, *d_tmask, *d_tables, *d_full, *d_ids, *d_cnt, *d_cursor,
+      *d_segs, *d_cand;
   gw::QueryView qv{};
 
   QuerySet(gw_ctx* ctx, bool use_ctx_buffers) {
-    gw_devbuf* b[10] = {&ctx->d_q_sources, &ctx->d_q_prefix, &ctx->d_q_idbase, &ctx->d_q_toff, &ctx->d_q_tmask,
-                        &ctx->d_q_tables, &ctx->d_q_full, &ctx->d_q_ids, &ctx->d_q_counts, &ctx->d_q_cursor};
-    gw_devbuf** d[10] = {&d_sources, &d_prefix, &d_id_base, &d_toff, &d_tmask,
-                         &d_tables, &d_full, &d_ids, &d_cnt, &d_cursor};
-    for (int i = 0; i < 10; ++i) *d[i] = use_ctx_buffers ? b[i] : &own[i];
+    gw_devbuf* b[12] = {&ctx->d_q_sources, &ctx->d_q_prefix, &ctx->d_q_idbase, &ctx->d_q_toff,
+                        &ctx->d_q_tmask,   &ctx->d_q_tables, &ctx->d_q_full,   &ctx->d_q_ids,
+                        &ctx->d_q_counts,  &ctx->d_q_cursor, &ctx->d_q_segs,   &ctx->d_q_cand};
+    gw_devbuf** d[12] = {&d_sources, &d_prefix, &d_id_base, &d_toff, &d_tmask, &d_tables,
+                         &d_full,    &d_ids,    &d_cnt,     &d_cursor, &d_segs, &d_cand};
+    for (int i = 0; i < 12; ++i) *d[i] = use_ctx_buffers ? b[i] : &own[i];
   }
   ~QuerySet() {
     for (auto& b : own) b.release();
@@ -83,6 +87,12 @@ gw_status upload_set(gw_ctx* ctx, QuerySet* s, uint32_t k, cudaStream_t st) {
   GW_CUDA(ctx, s->d_ids->ensure((uint64_t)n * k * 4), "top-k alloc");
   GW_CUDA(ctx, s->d_cnt->ensure((uint64_t)n * k * 4), "top-k alloc");
   GW_CUDA(ctx, s->d_cursor->ensure(sizeof(unsigned long long)), "query alloc");
+  s->seg_first.resize(n + 1);
+  s->seg_slots = gw::topk_segment_slots(n);
+  gw::topk_segment_prefix(s->tmask.data(), n, s->seg_slots, s->seg_first.data());
+  GW_CUDA(ctx, s->d_segs->ensure((n + 1) * 8), "top-k segments");
+  GW_CUDA(ctx, s->d_cand->ensure(s->seg_first[n] * k * 8 + 8), "top-k candidates");
+  GW_CUDA(ctx, cudaMemcpyAsync(s->d_segs->p, s->seg_first.data(), (n + 1) * 8, cudaMemcpyHostToDevice, st), "copy");
   GW_CUDA(ctx, cudaMemcpyAsync(s->d_sources->p, s->sources.data(), n * 4, cudaMemcpyHostToDevice, st), "copy");
   GW_CUDA(ctx, cudaMemcpyAsync(s->d_prefix->p, s->prefix.data(), (n + 1) * 8, cudaMemcpyHostToDevice, st), "copy");
   GW_CUDA(ctx, cudaMemcpyAsync(s->d_id_base->p, s->id_base.data(), n * 8, cudaMemcpyHostToDevice, st), "copy");
@@ -121,9 +131,12 @@ cudaError_t run_set(gw_ctx* ctx, const gw_walk_params* p, const gw::WalkArgs& a,
       e = gw::launch_walk_queries((int)p->rule, s->qv, 0, s->walks, ctx->view(), a, ctx->d_status.as<uint32_t>(),
                                   threads_per_sm, st);
     cudaEventRecord(ev[2], st);
-    if (e == cudaSuccess) e = gw::launch_topk(s->qv, 0, n, k, s->d_ids->as<uint32_t>(), s->d_cnt->as<uint32_t>(), st);
+    if (e == cudaSuccess)
+      e = gw::launch_topk_segmented(s->qv, 0, n, k, s->d_ids->as<uint32_t>(), s->d_cnt->as<uint32_t>(),
+                                    s->d_segs->as<unsigned long long>(), s->seg_first.data(), s->seg_slots,
+                                    s->d_cand->as<unsigned long long>(), st);
     cudaEventRecord(ev[3], st);
-    *launches += 3;
+    *launches += s->seg_first[n] > n ? 4 : 3;
   } else {
     cudaEventRecord(ev[1], st);
     for (uint32_t q = 0; q < n && e == cudaSuccess; ++q) {
@@ -131,7 +144,11 @@ cudaError_t run_set(gw_ctx* ctx, const gw_walk_params* p, const gw::WalkArgs& a,
       if (e == cudaSuccess)
         e = gw::launch_walk_queries((int)p->rule, s->qv, s->prefix[q], s->prefix[q + 1], ctx->view(), a,
                                     ctx->d_status.as<uint32_t>(), 0, st);
-      if (e == cudaSuccess) e = gw::launch_topk(s->qv, q, 1, k, s->d_ids->as<uint32_t>(), s->d_cnt->as<uint32_t>(), st);
+      if (e == cudaSuccess)
+        e = gw::launch_topk_segmented(s->qv, q, 1, k, s->d_ids->as<uint32_t>(), s->d_cnt->as<uint32_t>(),
+                                      s->d_segs->as<unsigned long long>(), s->seg_first.data(), s->seg_slots,
+                                      s->d_cand->as<unsigned long long>(), st);
+      *launches += s->seg_first[q + 1] - s->seg_first[q] > 1 ? 1 : 0;
     }
     cudaEventRecord(ev[2], st);
     cudaEventRecord(ev[3], st);
