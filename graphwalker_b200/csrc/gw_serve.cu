@@ -124,6 +124,7 @@ struct gw_server {
   gw_hostbuf h_stage;
   gw_devbuf d_stage;
   uint32_t stage_cap = 0;
+  gw_devbuf d_topk_segs, d_topk_cand;  // segmented top-k of large finishing tables
 };
 
 namespace {
@@ -274,8 +275,25 @@ bool superstep(gw_server* srv) {
   if (e == cudaSuccess)
     e = gw::launch_walk_queries((int)srv->params.rule, qv, 0, acc, ctx->view(), srv->args, d.status,
                                 ctx->ppr_threads_per_sm, st);
-  // queries whose last walks are in this superstep get their top-k now
-  if (e == cudaSuccess && nfin) e = gw::launch_topk(qv, 0, nfin, k, d.ids, d.counts, st);
+  // queries whose last walks are in this superstep get their top-k now; a
+  // large table is ranked by several CTAs (segmented top-k)
+  if (e == cudaSuccess && nfin) {
+    const uint32_t seg_slots = gw::topk_segment_slots(nfin);
+    std::vector<unsigned long long> sf(nfin + 1);
+    gw::topk_segment_prefix(h.tmask, nfin, seg_slots, sf.data());
+    if (sf[nfin] == nfin) {
+      e = gw::launch_topk(qv, 0, nfin, k, d.ids, d.counts, st);
+    } else {
+      e = srv->d_topk_segs.ensure((nfin + 1) * 8);
+      if (e == cudaSuccess) e = srv->d_topk_cand.ensure(sf[nfin] * k * 8);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(srv->d_topk_segs.p, sf.data(), (nfin + 1) * 8, cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess)
+        e = gw::launch_topk_segmented(qv, 0, nfin, k, d.ids, d.counts, srv->d_topk_segs.as<unsigned long long>(),
+                                      sf.data(), seg_slots, srv->d_topk_cand.as<unsigned long long>(), st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // sf is read by the copy above
+    }
+  }
   // status, flags and lists come back in one copy, then one synchronisation
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(h.status, d.status, 4 + (size_t)n * 4 + (size_t)n * k * 4 * 2, cudaMemcpyDeviceToHost, st);
@@ -497,6 +515,8 @@ gw_status gw_serve_close(gw_server* srv) {
   srv->tables.release();
   srv->h_stage.release();
   srv->d_stage.release();
+  srv->d_topk_segs.release();
+  srv->d_topk_cand.release();
   const gw_status s = srv->fatal;
   delete srv;
   return s;
