@@ -38,6 +38,7 @@ class WalkParams(Structure):
 
 SERVE_BATCHED, SERVE_PLAIN = 0, 1
 EDGE_RECORDS_OFF, EDGE_RECORDS_ON, EDGE_RECORDS_AUTO = 0, 1, 2
+FAULT_NONE, FAULT_DEVICE_ALLOC, FAULT_PINNED_ALLOC, FAULT_FILE_READ = 0, 1, 2, 3
 
 
 class ServeConfig(Structure):
@@ -144,6 +145,7 @@ _SIGS = {
     "gw_simrank_meet": (c_int32, [_P, _P, _P, c_uint32, c_uint32, _P, _P]),
     "gw_simrank_batch": (c_int32, [_P, POINTER(WalkParams), _P, _P, c_uint32, c_uint32, c_double, _P, _P]),
     "gw_convert_edgelist": (c_int32, [c_char_p, c_uint64, c_int32, POINTER(ConvertStats)]),
+    "gw_inject_fault": (c_int32, [c_uint32, c_uint32]),
 }
 
 _lib = None

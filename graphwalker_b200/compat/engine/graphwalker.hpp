@@ -163,6 +163,14 @@ class graphwalker_engine {
     gw_read_stats(ctx, &st);
     m.add_time("5_exec_updates", st.ms_total * 1e-3);
     if (st.block_loads) m.add("g_loadSubGraph", (double)st.block_loads, INTEGER);
+    // the device's own counters, in the same metrics map (graphwalker_metrics.txt)
+    m.add("gpu_walks", (double)st.walks, INTEGER);
+    m.add("gpu_supersteps", (double)st.supersteps, INTEGER);
+    m.add("gpu_block_loads", (double)st.block_loads, INTEGER);
+    m.add("gpu_bytes_h2d", (double)st.bytes_h2d, INTEGER);
+    m.add("gpu_ms_walk", st.ms_walk);
+    m.add("gpu_ms_partition", st.ms_partition);
+    m.add("gpu_ms_copy_wait", st.ms_copy_wait);
   }
 
   // Runs the walks in chunks that record paths on the device, then calls

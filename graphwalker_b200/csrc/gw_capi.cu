@@ -3,6 +3,7 @@
 #include <sys/stat.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cerrno>
 #include <cmath>
 #include <cstring>
@@ -51,6 +52,7 @@ gw_status read_pinned(gw_ctx* ctx, const std::string& path, gw_hostbuf* out, siz
     if (r == 0) break;
     got += r;
   }
+  if (n && gw::fault_now(GW_FAULT_FILE_READ)) got = n / 2;  // an injected short read
   fclose(f);
   if (got != n) return ctx->fail(GW_E_IO, "short read of %s (%zu of %zu bytes)", path.c_str(), got, n);
   *bytes = n;
@@ -205,6 +207,18 @@ gw_status status_of(gw_ctx* ctx, uint32_t st) {
   if (st & kStOverflow) return ctx->fail(GW_E_OVERFLOW, "a walk made more visits than path_stride");
   if (st & kStHops) return ctx->fail(GW_E_OVERFLOW, "an uncapped walk exceeded max_hops");
   return GW_OK;
+}
+
+namespace {
+std::atomic<uint32_t> g_fault_kind{GW_FAULT_NONE};
+std::atomic<int64_t> g_fault_countdown{0};
+}  // namespace
+
+bool fault_now(uint32_t kind) {
+  if (g_fault_kind.load(std::memory_order_relaxed) != kind) return false;
+  if (g_fault_countdown.fetch_sub(1) != 1) return false;
+  g_fault_kind.store(GW_FAULT_NONE);  // fires once
+  return true;
 }
 
 // Errors of entry points that have no context (gw_last_error(NULL)).
@@ -609,6 +623,14 @@ gw_status gw_simrank_batch(gw_ctx* ctx, const gw_walk_params* params, const uint
   }
   if (meet) std::copy(m.begin(), m.end(), meet);
   ctx->have_run = false;  // the path buffers now hold SimRank walks, not a gw_run's
+  return GW_OK;
+}
+
+gw_status gw_inject_fault(uint32_t kind, uint32_t after) {
+  if (kind > GW_FAULT_FILE_READ) return set_thread_error(GW_E_INVALID, "unknown fault kind");
+  gw::g_fault_kind.store(GW_FAULT_NONE);
+  gw::g_fault_countdown.store((int64_t)after + 1);
+  gw::g_fault_kind.store(kind);
   return GW_OK;
 }
 

@@ -8,12 +8,19 @@
 
 #include "gw_internal.h"
 
+namespace gw {
+// Host-side fault injection (gw_inject_fault): true when the calling
+// allocation or read of this kind is the one chosen to fail.
+bool fault_now(uint32_t kind);
+}  // namespace gw
+
 // A device allocation owned by the context.
 struct gw_devbuf {
   void* p = nullptr;
   size_t bytes = 0;
   cudaError_t ensure(size_t n) {
     if (n <= bytes && p) return cudaSuccess;
+    if (gw::fault_now(GW_FAULT_DEVICE_ALLOC)) return cudaErrorMemoryAllocation;
     if (p) cudaFree(p);
     p = nullptr;
     bytes = 0;
@@ -38,6 +45,7 @@ struct gw_hostbuf {
   size_t bytes = 0;
   cudaError_t ensure(size_t n) {
     if (n <= bytes && p) return cudaSuccess;
+    if (gw::fault_now(GW_FAULT_PINNED_ALLOC)) return cudaErrorMemoryAllocation;
     if (p) cudaFreeHost(p);
     p = nullptr;
     bytes = 0;
@@ -135,7 +143,7 @@ struct gw_ctx {
     return code;
   }
   gw_status cuda_fail(cudaError_t e, const char* what) {
-    return fail(GW_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return fail(e == cudaErrorMemoryAllocation ? GW_E_NOMEM : GW_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
   }
   gw::GraphView view() const {
     gw::GraphView g;

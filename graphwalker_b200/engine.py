@@ -38,6 +38,12 @@ def convert_edgelist(path: str, blocksize_kb: int = 0, device: int = 0) -> _lib.
     return st
 
 
+def inject_fault(kind: int, after: int = 0) -> None:
+    """Makes the after-th next host-side operation of `kind` fail once
+    (gw_inject_fault; FAULT_NONE disarms)."""
+    check(load().gw_inject_fault(kind, after))
+
+
 def simrank_estimate(meet, R: int, decay: float = 0.8) -> float:
     """SimRank estimate from first-meeting counts: sum_l meet[l] * decay^l / R^2
     (the quantity SimRank::computeResult sums, apps/simrank.cpp:71-84)."""

@@ -392,6 +392,19 @@ gw_status gw_convert_edgelist(const char *path, uint64_t blocksize_kb, int32_t d
 #define GW_EDGE_RECORDS_AUTO 2u
 gw_status gw_set_edge_records(gw_ctx *ctx, uint32_t mode, uint32_t *built);
 
+/* ---- failure injection (tests) ------------------------------------------ */
+/* Makes the `after`-th next host-side operation of one kind fail, once, in
+   this process: a device allocation by the engine (GW_E_NOMEM / GW_E_CUDA
+   from the call that needed it), a pinned host allocation, or a graph-file
+   read (a short read: GW_E_IO).  GW_FAULT_NONE disarms.  Nothing is done to
+   the GPU; a failed call leaves its context usable.  No counterpart in the
+   reference, whose failures are asserts (logger.hpp:215-217).              */
+#define GW_FAULT_NONE 0u
+#define GW_FAULT_DEVICE_ALLOC 1u
+#define GW_FAULT_PINNED_ALLOC 2u
+#define GW_FAULT_FILE_READ 3u
+gw_status gw_inject_fault(uint32_t kind, uint32_t after);
+
 /* ---- measurement -------------------------------------------------------- */
 /* Random 32-byte-sector gather microbenchmark over d_buf (n_words uint32):
    `loads` dependent-free random 4-byte loads; result in *sectors_per_s.     */

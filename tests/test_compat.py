@@ -128,6 +128,7 @@ def test_unchanged_rwdomination_graphlet_kkppr_apps(cuda_device, tmp_path):
     assert r.returncode == 0, r.stderr[-2000:]
     metrics = (tmp_path / "graphwalker_metrics.txt").read_text()
     assert "00_runtime=" in metrics and "5_exec_updates=" in metrics
+    assert "gpu_walks" in metrics and "gpu_ms_walk" in metrics  # the device's counters beside the reference's timers
     assert (tmp_path / "graphwalker_metrics.txt.statistics").read_text().strip()
     r = _run_app("graphlet", ["file", base, "N", "1024", "R", "5000", "L", "4", "blocksize_kb", kb], tmp_path)
     assert r.returncode == 0, r.stderr[-2000:]
