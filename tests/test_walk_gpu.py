@@ -237,3 +237,33 @@ def test_errors_surface_as_status_codes(cuda_device, oracle):
         # the context stays usable after device-reported errors
         G.run(gw.params(0, gw.SINK_VERTEX_COUNT, 10, seed=int(g["seed"])))
         assert G.read_counts().sum() == 12 * 10
+
+
+@pytest.mark.parametrize("rule,L", [(0, 10), (3, 6)])
+def test_checkpoint_and_resume_are_exact(cuda_device, oracle, rule, L):
+    """A superstep-boundary checkpoint (pending pools + counts) resumed in a
+    fresh context finishes with exactly the counts of an uninterrupted run:
+    every draw is keyed on (walk id, hop), so where a walk stopped does not
+    matter.  The reference's pools on disk are deleted at start and could not
+    serve as one (walk.hpp:50-51)."""
+    import graphwalker_b200 as gw
+    g = load_golden("rmat13")
+    seed = int(g["seed"])
+    cur = g["jump_cur"]
+    ids = np.arange(len(cur), dtype=np.uint32)
+    full = oracle.run_walks(g["rowptr"], g["colidx"], cur, ids=ids, src=cur, rule=rule, L=L, seed=seed)["counts"]
+    with _graph(g) as G:
+        G.walks_clear()
+        G.add_walks_at(cur, source=cur, ids=ids)
+        G.run(gw.params(rule, gw.SINK_VERTEX_COUNT, L, seed=seed, mode=gw.MODE_BLOCKED, max_supersteps=7))
+        part = G.read_counts().astype(np.int64)
+        pools = [G.read_pool(b) for b in range(G.nblocks)]
+    left = np.concatenate([p for p in pools if len(p)]) if any(len(p) for p in pools) else np.zeros((0, 4), np.uint32)
+    assert 0 < len(left) < len(cur)  # stopped mid-run
+    with _graph(g) as G2:  # resume in a new context
+        G2.walks_clear()
+        if len(left):
+            G2.add_walks_at(left[:, 0], source=left[:, 2], hop=left[:, 3], ids=left[:, 1])
+        G2.run(gw.params(rule, gw.SINK_VERTEX_COUNT, L, seed=seed))
+        rest = G2.read_counts().astype(np.int64)
+    assert np.array_equal(part + rest, full.astype(np.int64))
