@@ -20,6 +20,9 @@
 //   gw_residency    "hbm" (default) | "stream"
 //   gw_chunk        walks per device run in replay mode (default 4194304)
 //   gw_device       CUDA device ordinal (default 0)
+//   gw_edge_records "auto" (default): 16-byte edge records when they fit in
+//                   half of the free device memory | "on" | "off"
+//                   (gw_set_edge_records)
 #ifndef GRAPHWALKER_CMDOPTS_DEF
 #define GRAPHWALKER_CMDOPTS_DEF
 

@@ -60,6 +60,13 @@ class graphwalker_engine {
     if (gw_open(&d, &ctx) != GW_OK)
       logstream(LOG_FATAL) << "graphwalker_engine: " << gw_last_error(nullptr) << std::endl;
     m.stop_time("2_findSubGraph");
+    const std::string erec = get_option_string("gw_edge_records", "auto");
+    uint32_t erec_built = 0;
+    if (gw_set_edge_records(ctx, erec == "on" ? GW_EDGE_RECORDS_ON : erec == "off" ? GW_EDGE_RECORDS_OFF
+                                                                                     : GW_EDGE_RECORDS_AUTO,
+                            &erec_built) != GW_OK)
+      logstream(LOG_FATAL) << "graphwalker_engine: " << gw_last_error(ctx) << std::endl;
+    m.set("gpu_edge_records", std::string(erec_built ? "on" : "off"));
     uint32_t nv = 0, nb = 0;
     uint64_t ne = 0;
     gw_graph_info(ctx, &nv, &ne, &nb);
