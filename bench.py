@@ -701,7 +701,8 @@ def ooc_arm(args) -> None:
         res[name] = {"ms": st.ms_total, "walk_steps_per_s": nv * L / (st.ms_total * 1e-3),
                      "supersteps": int(st.supersteps), "block_loads": int(st.block_loads),
                      "h2d_GB": st.bytes_h2d / 1e9,
-                     "h2d_GBps": st.bytes_h2d / (st.ms_total * 1e-3) / 1e9 if st.bytes_h2d else 0.0}
+                     "h2d_GBps": st.bytes_h2d / (st.ms_total * 1e-3) / 1e9 if st.bytes_h2d else 0.0,
+                     "device_ms": {"walk": st.ms_walk, "partition": st.ms_partition, "copy_wait": st.ms_copy_wait}}
         print(json.dumps({name: res[name]}), flush=True)
     s = res["streamed_blocked"]
     line = {"metric": "walk-steps/s", "value": s["walk_steps_per_s"], "unit": "walk-steps/s", "workload": "ooc",

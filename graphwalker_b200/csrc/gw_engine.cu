@@ -204,9 +204,21 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     return victim;
   };
 
-  cudaEvent_t t0, t1;
-  cudaEventCreate(&t0);
-  cudaEventCreate(&t1);
+  // run start/end, and the phases of each superstep (read after its own
+  // synchronisation): ph[0] before the copy wait, ph[1] walk start, ph[2]
+  // walk end, ph[3] partition end.  Destroyed on every return.
+  struct Events {
+    cudaEvent_t e[6];
+    Events() {
+      for (auto& x : e) cudaEventCreate(&x);
+    }
+    ~Events() {
+      for (auto& x : e) cudaEventDestroy(x);
+    }
+  } evs;
+  cudaEvent_t t0 = evs.e[0], t1 = evs.e[1];
+  cudaEvent_t* ph = evs.e + 2;
+  double ms_walk = 0, ms_partition = 0, ms_copy_wait = 0;
   cudaEventRecord(t0, st);
   uint64_t superstep = 0;
   cudaError_t e = cudaSuccess;
@@ -222,6 +234,7 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     const unsigned long long* beg_pos = nullptr;
     const uint32_t* csr = nullptr;
     int slot = -1;
+    cudaEventRecord(ph[0], st);
     if (streaming) {
       slot = load_block(b, -1);
       cudaStreamWaitEvent(st, slots.ready[slot], 0);
@@ -230,10 +243,12 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     }
     // ---- exec_updates ----
     GW_CUDA(ctx, ctx->d_dest.ensure(n * 4), "dest alloc");
+    cudaEventRecord(ph[1], st);
     e = launch_walk_block((int)p->rule, (int)p->sink, p->aggregate != 0, ctx->pools[b].as<gw_walk_rec>(),
                           n, ctx->view(), beg_pos, csr, ab, sv, ctx->d_blocks.as<uint32_t>(), nb,
                           ctx->d_dest.as<uint32_t>(), ctx->d_status.as<uint32_t>(), st);
     if (e != cudaSuccess) break;
+    cudaEventRecord(ph[2], st);
     if (streaming) {
       cudaEventRecord(slots.free_ev[slot], st);
       // prefetch the block most likely chosen next while this one runs
@@ -297,8 +312,18 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
                                    ctx->d_out_ptr.as<gw_walk_rec* const>(),
                                    ctx->d_out_base.as<uint64_t>(), st);
     if (e != cudaSuccess) break;
+    cudaEventRecord(ph[3], st);
     // the pinned up-copies must land before h_ptr/h_base are rewritten
     e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) {
+      float a = 0.f, w = 0.f, q = 0.f;
+      cudaEventElapsedTime(&a, ph[0], ph[1]);
+      cudaEventElapsedTime(&w, ph[1], ph[2]);
+      cudaEventElapsedTime(&q, ph[2], ph[3]);
+      ms_copy_wait += a;
+      ms_walk += w;
+      ms_partition += q;
+    }
     uint64_t forwarded = 0;
     for (uint32_t d = 0; d < nb; ++d) {
       if (!h_totals[d]) continue;
@@ -312,18 +337,15 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     ++superstep;
   }
   cudaEventRecord(t1, st);
-  if (e != cudaSuccess) {
-    cudaEventDestroy(t0);
-    cudaEventDestroy(t1);
-    return ctx->cuda_fail(e, "blocked engine");
-  }
+  if (e != cudaSuccess) return ctx->cuda_fail(e, "blocked engine");
   s = take_status(ctx, st);
   float ms = 0.f;
   cudaEventElapsedTime(&ms, t0, t1);
-  cudaEventDestroy(t0);
-  cudaEventDestroy(t1);
   ctx->stats.supersteps = superstep;
   ctx->stats.ms_total = ms;
+  ctx->stats.ms_walk = ms_walk;
+  ctx->stats.ms_partition = ms_partition;
+  ctx->stats.ms_copy_wait = ms_copy_wait;
   ctx->last_nwalks = nwalks;
   ctx->last_sink = p->sink;
   ctx->last_stride = 0;
