@@ -334,6 +334,9 @@ def our_arm(args) -> None:
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     p = gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, L, seed=args.walk_seed, aggregate=bool(args.aggregate))
 
+    # launch shape (CTAs per SM) timed on these walks before the warm-up
+    tuned_ctas = G.walk_autotune(p, walks, nv)
+
     def step():
         counts.zero_()
         G.walk_device(p, walks, nv, counts=counts, stream=sh)
@@ -451,7 +454,8 @@ def our_arm(args) -> None:
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
             "warmup": max(3, args.warmup), "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {**workload_config(args, G.nblocks), "graph_layout": layout},
+            "config": {**workload_config(args, G.nblocks), "graph_layout": layout,
+                       "autotuned_ctas_per_sm": tuned_ctas},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": K, "clocks": clk.summary(),
             "walk_steps_per_step": steps_per_launch * world}
     G.close()

@@ -146,6 +146,7 @@ _SIGS = {
     "gw_simrank_batch": (c_int32, [_P, POINTER(WalkParams), _P, _P, c_uint32, c_uint32, c_double, _P, _P]),
     "gw_convert_edgelist": (c_int32, [c_char_p, c_uint64, c_int32, POINTER(ConvertStats)]),
     "gw_inject_fault": (c_int32, [c_uint32, c_uint32]),
+    "gw_walk_autotune": (c_int32, [_P, POINTER(WalkParams), _P, c_uint64, POINTER(c_uint32)]),
 }
 
 _lib = None

@@ -224,6 +224,16 @@ bool fault_now(uint32_t kind) {
 // Errors of entry points that have no context (gw_last_error(NULL)).
 gw_status thread_error(gw_status code, const std::string& msg) { return set_thread_error(code, msg); }
 
+// Grid of a resident walk launch over n walks: the autotuned CTAs per SM
+// (gw_walk_autotune), or 0 for the kernel's full occupancy.
+int resident_grid(gw_ctx* ctx, uint64_t n) {
+  if (ctx->walk_ctas_per_sm <= 0) return 0;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  const uint64_t need = (n + kWalkThreads - 1) / kWalkThreads, full = (uint64_t)sms * ctx->walk_ctas_per_sm;
+  return (int)(need < full ? (need ? need : 1) : full);
+}
+
 }  // namespace gw
 
 extern "C" {
@@ -744,7 +754,8 @@ gw_status gw_run(gw_ctx* ctx, const gw_walk_params* params) {
   const bool use_win = params->sink == GW_SINK_VERTEX_COUNT && ctx->counts_window(sv.counts, &win);
   cudaError_t e = gw::launch_walk_resident((int)params->rule, (int)params->sink, params->aggregate != 0,
                                            ctx->d_walks.as<gw_walk_rec>(), n, ctx->view(), a, sv,
-                                           ctx->d_status.as<uint32_t>(), 0, st, use_win ? &win : nullptr);
+                                           ctx->d_status.as<uint32_t>(), gw::resident_grid(ctx, n), st,
+                                           use_win ? &win : nullptr);
   cudaEventRecord(e1, st);
   if (e != cudaSuccess) {
     cudaEventDestroy(e0);
@@ -869,7 +880,8 @@ gw_status gw_run_pools(gw_ctx* ctx, const gw_walk_params* params, const uint64_t
     if (e == cudaSuccess)
       e = gw::launch_walk_resident((int)params->rule, (int)params->sink, params->aggregate != 0,
                                    ctx->d_walks.as<gw_walk_rec>() + lo, m, ctx->view(), a, sv,
-                                   ctx->d_status.as<uint32_t>(), 0, cs, use_win ? &win : nullptr);
+                                   ctx->d_status.as<uint32_t>(), gw::resident_grid(ctx, m), cs,
+                                   use_win ? &win : nullptr);
   }
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(counts, ctx->d_counts.p, (size_t)ctx->nv * 4, cudaMemcpyDeviceToHost, cs);
@@ -908,9 +920,68 @@ gw_status gw_walk_device(gw_ctx* ctx, const gw_walk_params* params, const gw_wal
   const bool use_win = params->sink == GW_SINK_VERTEX_COUNT && ctx->counts_window(d_counts, &win);
   cudaError_t e = gw::launch_walk_resident((int)params->rule, (int)params->sink, params->aggregate != 0,
                                            d_walks, n, ctx->view(), a, sv,
-                                           ctx->d_status.as<uint32_t>(), 0, st, use_win ? &win : nullptr);
+                                           ctx->d_status.as<uint32_t>(), gw::resident_grid(ctx, n), st,
+                                           use_win ? &win : nullptr);
   if (e != cudaSuccess) return ctx->cuda_fail(e, "walk kernel launch");
   return GW_OK;
+}
+
+gw_status gw_walk_autotune(gw_ctx* ctx, const gw_walk_params* params, const gw_walk_rec* d_walks, uint64_t n,
+                           uint32_t* ctas_per_sm) {
+  if (!ctx) return set_thread_error(GW_E_INVALID, "NULL context");
+  if (ctx->residency != GW_RESIDENT_HBM) return ctx->fail(GW_E_STATE, "gw_walk_autotune needs a resident graph");
+  if (!d_walks || n == 0) return ctx->fail(GW_E_INVALID, "gw_walk_autotune: no walks");
+  gw_walk_params pp = *params;  // counts into a scratch array; other sinks cost the same per step
+  pp.sink = GW_SINK_VERTEX_COUNT;
+  gw::WalkArgs a;
+  gw_status s = gw::make_walk_args(ctx, &pp, &a);
+  if (s != GW_OK) return s;
+  GW_CUDA(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  GW_CUDA(ctx, ctx->d_counts.ensure((size_t)ctx->nv * 4), "counts alloc");
+  gw::SinkView sv{};
+  sv.counts = ctx->d_counts.as<uint32_t>();
+  cudaStream_t st = ctx->stream;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  const int full = gw::walk_resident_grid((int)pp.rule, (int)pp.sink, pp.aggregate != 0, (uint64_t)sms * 64 * 1024);
+  const int max_per_sm = std::max(1, full / sms);
+  cudaAccessPolicyWindow win;
+  const bool use_win = ctx->counts_window(sv.counts, &win);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int best = max_per_sm;
+  float best_ms = 1e30f;
+  for (int c = std::max(1, max_per_sm / 2); c <= max_per_sm; ++c) {
+    ctx->walk_ctas_per_sm = c;
+    float sum = 0.f;
+    for (int rep = 0; rep < 4; ++rep) {
+      cudaEventRecord(e0, st);
+      cudaError_t e = gw::launch_walk_resident((int)pp.rule, (int)pp.sink, pp.aggregate != 0, d_walks, n, ctx->view(),
+                                               a, sv, ctx->d_status.as<uint32_t>(), gw::resident_grid(ctx, n), st,
+                                               use_win ? &win : nullptr);
+      cudaEventRecord(e1, st);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      if (e != cudaSuccess) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        ctx->walk_ctas_per_sm = 0;
+        return ctx->cuda_fail(e, "autotune launch");
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep) sum += ms;  // the first run warms up
+    }
+    if (sum < best_ms) {
+      best_ms = sum;
+      best = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ctx->walk_ctas_per_sm = best == max_per_sm ? 0 : best;  // full occupancy is the default shape
+  if (ctas_per_sm) *ctas_per_sm = (uint32_t)best;
+  return gw::take_status(ctx, st);
 }
 
 gw_status gw_set_l2_fetch_granularity(gw_ctx* ctx, uint32_t bytes, uint32_t* previous) {

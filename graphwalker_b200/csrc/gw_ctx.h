@@ -113,6 +113,7 @@ struct gw_ctx {
   gw_devbuf d_q_sources, d_q_prefix, d_q_idbase, d_q_toff, d_q_tmask, d_q_tables, d_q_full, d_q_ids,
       d_q_counts, d_q_visits, d_q_cursor, d_q_segs, d_q_cand;
   int ppr_threads_per_sm = 0;  // autotuned launch shape (0 = full occupancy)
+  int walk_ctas_per_sm = 0;    // autotuned resident-walk launch shape (0 = full occupancy)
   uint32_t ppr_chunk = 0;      // autotuned walks per cursor grab (0 = default)
 
   std::string err;
@@ -159,6 +160,8 @@ struct gw_ctx {
 namespace gw {
 // Records an error of an entry point without a context (gw_last_error(NULL)).
 gw_status thread_error(gw_status code, const std::string& msg);
+// Grid of a resident walk launch over n walks (the context's tuned shape).
+int resident_grid(gw_ctx* ctx, uint64_t n);
 // Fills launch constants from the API parameters; validates them.
 gw_status make_walk_args(gw_ctx* ctx, const gw_walk_params* p, WalkArgs* a);
 // Reads and clears the device status word (synchronises ctx->stream).

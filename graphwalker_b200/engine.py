@@ -270,6 +270,13 @@ class Graph:
               self._h)
         return scores, meet
 
+    def walk_autotune(self, p: WalkParams, walks, n: int) -> int:
+        """CTAs per SM chosen for this graph's later resident walk launches
+        (gw_walk_autotune), timed on the given device walks."""
+        out = c_uint32()
+        check(load().gw_walk_autotune(self._h, byref(p), _ptr(walks), n, byref(out)), self._h)
+        return out.value
+
     def sync(self, stream: int | None = None) -> None:
         check(load().gw_sync(self._h, stream), self._h)
 

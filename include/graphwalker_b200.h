@@ -297,6 +297,14 @@ gw_status gw_pack_words_device(gw_ctx *ctx, const gw_walk_rec *d_walks, uint64_t
                                uint64_t *d_words, uint32_t *d_blocks, void *stream);
 /* Synchronises the stream and returns the device status of earlier kernels. */
 gw_status gw_sync(gw_ctx *ctx, void *stream);
+/* Times the resident walk kernel on the caller's device walks (counts into a
+   scratch array of the context) at each occupancy from half to full CTAs per
+   SM, and keeps the fastest for this context's later resident launches
+   (gw_run, gw_run_pools, gw_walk_device).  The choice changes no result.
+   *ctas_per_sm (may be NULL) receives it.  (The reference has no tuner;
+   its update loop is an OpenMP loop, graphwalker.hpp:257-270.)            */
+gw_status gw_walk_autotune(gw_ctx *ctx, const gw_walk_params *params, const gw_walk_rec *d_walks, uint64_t n,
+                           uint32_t *ctas_per_sm);
 /* SimRank's meeting reduction (replaces the O(R^2 L) host loop of
    SimRank::computeResult, apps/simrank.cpp:71-84).  d_paths_a / d_paths_b:
    R walks of L visits each, row-major (walk i = row i), 0xFFFFFFFF = no

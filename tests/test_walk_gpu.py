@@ -267,3 +267,24 @@ def test_checkpoint_and_resume_are_exact(cuda_device, oracle, rule, L):
         G2.run(gw.params(rule, gw.SINK_VERTEX_COUNT, L, seed=seed))
         rest = G2.read_counts().astype(np.int64)
     assert np.array_equal(part + rest, full.astype(np.int64))
+
+
+def test_walk_autotune_keeps_results(cuda_device, oracle):
+    """The tuned launch shape of the resident kernel changes no count."""
+    import torch
+
+    import graphwalker_b200 as gw
+    rp, ci = oracle.rmat_csr(16, 16, seed=2)
+    nv = len(rp) - 1
+    cur = np.arange(nv, dtype=np.uint32)
+    ref = oracle.run_walks(rp, ci, cur, ids=cur, src=cur, rule=0, L=10, seed=8)["counts"]
+    with gw.Graph.from_csr(rp, ci, oracle.compute_blocks(rp, 512)) as G:
+        v = torch.arange(nv, dtype=torch.int64, device="cuda")
+        walks = torch.stack([v, v, v, torch.zeros_like(v)], dim=1).to(torch.int32).contiguous()
+        p = gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, 10, seed=8)
+        c = G.walk_autotune(p, walks, nv)
+        assert 1 <= c <= 8
+        counts = torch.zeros(nv, dtype=torch.int32, device="cuda")
+        G.walk_device(p, walks, nv, counts=counts)
+        G.sync()
+        assert np.array_equal(counts.cpu().numpy().view(np.uint32), ref)
