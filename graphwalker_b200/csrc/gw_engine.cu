@@ -204,24 +204,45 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     return victim;
   };
 
-  // run start/end, and the phases of each superstep (read after its own
-  // synchronisation): ph[0] before the copy wait, ph[1] walk start, ph[2]
-  // walk end, ph[3] partition end.  Destroyed on every return.
+  double ms_walk = 0, ms_partition = 0, ms_copy_wait = 0;
+  // run start/end, and the phases of each superstep in two alternating sets
+  // (a superstep's set is read after the next superstep's synchronisation):
+  // ph[0] before the copy wait, ph[1] walk start, ph[2] walk end, ph[3]
+  // partition end.  Destroyed on every return; so are the pools that grown
+  // pools replaced, once no queued copy reads them.
   struct Events {
-    cudaEvent_t e[6];
+    cudaEvent_t e[10];
+    std::vector<void*> retired;
     Events() {
       for (auto& x : e) cudaEventCreate(&x);
     }
     ~Events() {
       for (auto& x : e) cudaEventDestroy(x);
+      for (void* p : retired) cudaFree(p);
     }
   } evs;
   cudaEvent_t t0 = evs.e[0], t1 = evs.e[1];
-  cudaEvent_t* ph = evs.e + 2;
-  double ms_walk = 0, ms_partition = 0, ms_copy_wait = 0;
+  auto phase_set = [&](uint64_t step) { return evs.e + 2 + 4 * (step & 1); };
+  auto add_phases = [&](uint64_t step) {
+    cudaEvent_t* q = phase_set(step);
+    float a = 0.f, w = 0.f, m = 0.f;
+    cudaEventElapsedTime(&a, q[0], q[1]);
+    cudaEventElapsedTime(&w, q[1], q[2]);
+    cudaEventElapsedTime(&m, q[2], q[3]);
+    ms_copy_wait += a;
+    ms_walk += w;
+    ms_partition += m;
+  };
+  // Grown pools come from the stream-ordered allocator, so replacing one
+  // queues its free behind the copy out of it; a pool from gw_walks_add is
+  // retired instead and freed with the events.
+  std::vector<char> pool_async(nb, 0);
   cudaEventRecord(t0, st);
   uint64_t superstep = 0;
   cudaError_t e = cudaSuccess;
+  // The scatter of superstep k is left queued: the host next waits on the
+  // stream for the partition totals of superstep k + 1, which orders it.
+  bool pending = false;
   while (walksum > 0 && e == cudaSuccess &&
          (p->max_supersteps == 0 || superstep < p->max_supersteps)) {
     const uint32_t b = choose_block(ctx->pool_size, ctx->minstep, p->prob, p->seed, superstep);
@@ -234,6 +255,19 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     const unsigned long long* beg_pos = nullptr;
     const uint32_t* csr = nullptr;
     int slot = -1;
+    const PartitionPlan plan = partition_plan(n, nbk);
+    const size_t hist_n = (size_t)plan.nbuckets * plan.ntiles;
+    if (pending && (n * 4 > ctx->d_dest.bytes || hist_n * 4 > ctx->d_tile_hist.bytes ||
+                    hist_n * 4 > ctx->d_tile_off.bytes || plan.scan_temp_bytes > ctx->d_scan_temp.bytes)) {
+      // a buffer the queued scatter reads is about to be replaced
+      e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) break;
+    }
+    GW_CUDA(ctx, ctx->d_dest.ensure(n * 4), "dest alloc");
+    GW_CUDA(ctx, ctx->d_tile_hist.ensure(hist_n * 4), "hist alloc");
+    GW_CUDA(ctx, ctx->d_tile_off.ensure(hist_n * 4), "hist alloc");
+    GW_CUDA(ctx, ctx->d_scan_temp.ensure(plan.scan_temp_bytes), "scan alloc");
+    cudaEvent_t* ph = phase_set(superstep);
     cudaEventRecord(ph[0], st);
     if (streaming) {
       slot = load_block(b, -1);
@@ -242,7 +276,6 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
       csr = slots.csr[slot].as<uint32_t>();
     }
     // ---- exec_updates ----
-    GW_CUDA(ctx, ctx->d_dest.ensure(n * 4), "dest alloc");
     cudaEventRecord(ph[1], st);
     e = launch_walk_block((int)p->rule, (int)p->sink, p->aggregate != 0, ctx->pools[b].as<gw_walk_rec>(),
                           n, ctx->view(), beg_pos, csr, ab, sv, ctx->d_blocks.as<uint32_t>(), nb,
@@ -262,11 +295,6 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
       if (nxt != kNoBlock && slots.slot_of[nxt] < 0 && nslots > 1) load_block(nxt, slot);
     }
     // ---- moveWalk: stable partition by destination block ----
-    const PartitionPlan plan = partition_plan(n, nbk);
-    const size_t hist_n = (size_t)plan.nbuckets * plan.ntiles;
-    GW_CUDA(ctx, ctx->d_tile_hist.ensure(hist_n * 4), "hist alloc");
-    GW_CUDA(ctx, ctx->d_tile_off.ensure(hist_n * 4), "hist alloc");
-    GW_CUDA(ctx, ctx->d_scan_temp.ensure(plan.scan_temp_bytes), "scan alloc");
     uint32_t* d_tot = ctx->d_totals.as<uint32_t>();
     uint32_t* d_minhop = d_tot + nbk;
     GW_CUDA(ctx, cudaMemsetAsync(d_minhop, 0xff, nbk * 4, st), "minhop clear");
@@ -279,6 +307,7 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
       e = cudaMemcpyAsync(h_totals, d_tot, 2 * nbk * 4, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) break;
+    if (superstep > 0) add_phases(superstep - 1);
     // updateWalkNum: grow destination pools, then scatter into them
     for (uint32_t d = 0; d < nb; ++d) {
       const uint64_t need = ctx->pool_size[d] + h_totals[d];
@@ -286,16 +315,22 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
         uint64_t ncap = std::max<uint64_t>(need, cap[d] * 2);
         ncap = std::max<uint64_t>(ncap, 1024);
         void* np = nullptr;
-        e = cudaMalloc(&np, ncap * sizeof(gw_walk_rec));
+        e = cudaMallocAsync(&np, ncap * sizeof(gw_walk_rec), st);
         if (e != cudaSuccess) break;
         if (ctx->pool_size[d])
           e = cudaMemcpyAsync(np, ctx->pools[d].p, ctx->pool_size[d] * sizeof(gw_walk_rec),
                               cudaMemcpyDeviceToDevice, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (ctx->pools[d].p) cudaFree(ctx->pools[d].p);
+        if (ctx->pools[d].p) {
+          if (pool_async[d])
+            cudaFreeAsync(ctx->pools[d].p, st);
+          else
+            evs.retired.push_back(ctx->pools[d].p);
+        }
+        pool_async[d] = 1;
         ctx->pools[d].p = np;
         ctx->pools[d].bytes = ncap * sizeof(gw_walk_rec);
         cap[d] = ncap;
+        if (e != cudaSuccess) break;
       }
       h_ptr[d] = ctx->pools[d].as<gw_walk_rec>();
       h_base[d] = ctx->pool_size[d];
@@ -313,17 +348,9 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
                                    ctx->d_out_base.as<uint64_t>(), st);
     if (e != cudaSuccess) break;
     cudaEventRecord(ph[3], st);
-    // the pinned up-copies must land before h_ptr/h_base are rewritten
-    e = cudaStreamSynchronize(st);
-    if (e == cudaSuccess) {
-      float a = 0.f, w = 0.f, q = 0.f;
-      cudaEventElapsedTime(&a, ph[0], ph[1]);
-      cudaEventElapsedTime(&w, ph[1], ph[2]);
-      cudaEventElapsedTime(&q, ph[2], ph[3]);
-      ms_copy_wait += a;
-      ms_walk += w;
-      ms_partition += q;
-    }
+    // h_ptr/h_base are rewritten only after the next totals wait, when these
+    // up-copies have landed
+    pending = true;
     uint64_t forwarded = 0;
     for (uint32_t d = 0; d < nb; ++d) {
       if (!h_totals[d]) continue;
@@ -338,7 +365,8 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
   }
   cudaEventRecord(t1, st);
   if (e != cudaSuccess) return ctx->cuda_fail(e, "blocked engine");
-  s = take_status(ctx, st);
+  s = take_status(ctx, st);  // synchronises the stream
+  if (superstep > 0) add_phases(superstep - 1);
   float ms = 0.f;
   cudaEventElapsedTime(&ms, t0, t1);
   ctx->stats.supersteps = superstep;
