@@ -115,6 +115,10 @@ struct gw_ctx {
   int ppr_threads_per_sm = 0;  // autotuned launch shape (0 = full occupancy)
   int walk_ctas_per_sm = 0;    // autotuned resident-walk launch shape (0 = full occupancy)
   uint32_t ppr_chunk = 0;      // autotuned walks per cursor grab (0 = default)
+  // Batch tags of d_q_tables: the next tag, and whether every slot is empty
+  // or carries a tag below it.
+  uint32_t q_tag_next = 0;
+  bool q_tags_ok = false;
 
   std::string err;
 

@@ -7,8 +7,11 @@
 // walks are the same whether it runs alone or inside any batch.
 //
 // Visits go to a per-query open-addressing table of 64-bit slots
-// (vertex << 32 | count; all-ones = empty) -- the sparse replacement of
-// msppr's per-source DiscreteDistribution (discretedistribution.hpp:44-57).
+// ((tag | vertex) << 32 | count; all-ones = empty) -- the sparse replacement
+// of msppr's per-source DiscreteDistribution (discretedistribution.hpp:44-57).
+// The tag, in the vertex word's bits above the largest vertex id, names the
+// batch that wrote the slot: a batch treats the slots of earlier batches as
+// free, so its tables need no clearing pass.
 // Lanes of a warp that visit the same (query, vertex) in the same step are
 // folded into one table update, and the hop-0 visits of a query's walks (all
 // at its source) are added in one update.  Warps take walks in small chunks
@@ -66,35 +69,48 @@ __device__ __forceinline__ void red_add_u64(unsigned long long* a, unsigned long
                : "memory");
 }
 
-// Completes a table update whose first probe (a CAS at slot s) returned
-// `old`: nothing to do if the CAS claimed the slot, an add if the slot holds
-// v, otherwise linear probing from s + 1.  False when the table is full (no
-// free slot or slot holding v within kMaxProbes of s).
+// A slot another batch wrote (or never written): free for this one.
+__device__ __forceinline__ bool slot_free(unsigned long long old, uint32_t tag, uint32_t tag_mask) {
+  return old == kEmptySlot || ((uint32_t)(old >> 32) & tag_mask) != tag;
+}
+
+// Completes a table update of n visits under key = tag | v whose first probe
+// (a CAS of the empty pattern at slot s) returned `old`: nothing to do if the
+// CAS claimed the slot, an add if the slot holds the key; a slot left by an
+// earlier batch is claimed by a second CAS against its content (within a
+// batch only current keys are written, so a slot is resolved in at most two
+// CAS); otherwise linear probing from s + 1.  False when the table is full
+// (no free slot or slot holding the key within kMaxProbes of s).
 __device__ __forceinline__ bool table_finish(unsigned long long* __restrict__ t, uint32_t mask, uint32_t s,
-                                             unsigned long long old, uint32_t v, uint32_t n, uint64_t pol) {
-  if (old == kEmptySlot) return true;
-  if ((uint32_t)(old >> 32) == v) {
-    red_add_u64(t + s, n, pol);
-    return true;
-  }
+                                             unsigned long long old, uint32_t key, uint32_t n, uint64_t pol,
+                                             uint32_t tag_mask) {
+  const unsigned long long val = ((unsigned long long)key << 32) | n;
+  unsigned long long cmp = kEmptySlot;
   const uint32_t last = probe_limit(mask);
-  for (uint32_t probe = 1; probe <= last; ++probe) {
-    s = (s + 1) & mask;
-    old = cas_u64(t + s, kEmptySlot, ((unsigned long long)v << 32) | n);
-    if (old == kEmptySlot) return true;
-    if ((uint32_t)(old >> 32) == v) {
+  for (uint32_t probe = 0;;) {
+    if (old == cmp) return true;
+    if ((uint32_t)(old >> 32) == key) {
       red_add_u64(t + s, n, pol);
       return true;
     }
+    if (slot_free(old, key & tag_mask, tag_mask)) {
+      cmp = old;
+      old = cas_u64(t + s, cmp, val);
+      continue;
+    }
+    if (++probe > last) return false;
+    s = (s + 1) & mask;
+    cmp = kEmptySlot;
+    old = cas_u64(t + s, cmp, val);
   }
-  return false;
 }
 
-// Adds n visits of vertex v to a table; false when the table is full.
-__device__ __forceinline__ bool table_add(unsigned long long* __restrict__ t, uint32_t mask, uint32_t v,
-                                          uint32_t n, uint64_t pol) {
-  const uint32_t s = slot_hash(v) & mask;
-  return table_finish(t, mask, s, cas_u64(t + s, kEmptySlot, ((unsigned long long)v << 32) | n), v, n, pol);
+// Adds n visits under key = tag | v to a table; false when the table is full.
+__device__ __forceinline__ bool table_add(unsigned long long* __restrict__ t, uint32_t mask, uint32_t key,
+                                          uint32_t n, uint64_t pol, uint32_t tag_mask) {
+  const uint32_t s = slot_hash(key & ~tag_mask) & mask;
+  return table_finish(t, mask, s, cas_u64(t + s, kEmptySlot, ((unsigned long long)key << 32) | n), key, n, pol,
+                      tag_mask);
 }
 
 __device__ __forceinline__ uint32_t query_of(const unsigned long long* __restrict__ prefix, uint32_t nq,
@@ -158,8 +174,8 @@ __global__ void __launch_bounds__(kPprThreads)
         }
         const unsigned long long lo = q_lo > w_begin ? q_lo : w_begin, hi = q_hi < w_end ? q_hi : w_end;
         if (visits_source && j == lo && src < g.nv &&
-            !table_add(qv.tables + __ldg(qv.table_off + q), __ldg(qv.table_mask + q), src, (uint32_t)(hi - lo),
-                       hp.cnt))
+            !table_add(qv.tables + __ldg(qv.table_off + q), __ldg(qv.table_mask + q), qv.tag | src,
+                       (uint32_t)(hi - lo), hp.cnt, qv.tag_mask))
           qv.full[q] = 1u;
         v = src;
         cur_rec = src_rec;
@@ -199,7 +215,7 @@ __global__ void __launch_bounds__(kPprThreads)
           mask = __ldg(qv.table_mask + q);
           s0 = slot_hash(v) & mask;
           prefetch_slot(t + s0);  // keeps the table's lines in L2 ahead of the graph's (walk phase -34 %)
-          old = cas_u64(t + s0, kEmptySlot, ((unsigned long long)v << 32) | n);
+          old = cas_u64(t + s0, kEmptySlot, ((unsigned long long)(qv.tag | v) << 32) | n);
         }
       }
       // the hop itself: hop_advance_rec's draws and choices, written out so
@@ -236,7 +252,7 @@ __global__ void __launch_bounds__(kPprThreads)
           moved = false;
         }
       }
-      if (leader && !table_finish(t, mask, s0, old, v, n, hp.cnt)) qv.full[q] = 1u;
+      if (leader && !table_finish(t, mask, s0, old, qv.tag | v, n, hp.cnt, qv.tag_mask)) qv.full[q] = 1u;
       end = !moved;
       if (moved) {
         v = next;
@@ -299,7 +315,7 @@ __device__ void block_best(Src src, uint32_t n, uint32_t k, unsigned long long* 
     }
 #pragma unroll
     for (uint32_t u = 0; u < kTopkUnroll; ++u) {
-      const unsigned long long key = Src::key(raw[u]);
+      const unsigned long long key = src.key(raw[u]);
       if (key > thresh) {
         const uint32_t pos = atomicAdd(&ncand, 1u);
         cand[pos] = key;  // room for one full round is kept free below
@@ -321,14 +337,16 @@ __device__ void block_best(Src src, uint32_t n, uint32_t k, unsigned long long* 
 }
 
 // Key of a table slot: count << 32 | ~vertex (larger = more visits, then the
-// smaller vertex id); 0 for an empty slot.
+// smaller vertex id); 0 for a free slot (empty, or another batch's).
 struct SlotKey {
   static constexpr unsigned long long kNone = kEmptySlot;
   const unsigned long long* t;
   uint64_t pol;
+  uint32_t tag, tag_mask;
   __device__ unsigned long long fetch(uint32_t i) const { return ld_nc_u64(t + i, pol); }
-  __device__ static unsigned long long key(unsigned long long e) {
-    return e == kEmptySlot ? 0ull : ((e & 0xffffffffull) << 32) | (uint32_t)~(uint32_t)(e >> 32);
+  __device__ unsigned long long key(unsigned long long e) const {
+    return slot_free(e, tag, tag_mask) ? 0ull
+                                       : ((e & 0xffffffffull) << 32) | (uint32_t)~((uint32_t)(e >> 32) & ~tag_mask);
   }
 };
 
@@ -356,8 +374,8 @@ __global__ void __launch_bounds__(kTopkThreads)
   __shared__ uint32_t ncand;
   __shared__ unsigned long long thresh;
   const uint32_t q = q_begin + blockIdx.x;
-  block_best(SlotKey{qv.tables + qv.table_off[q], l2_policy(true, false)}, qv.table_mask[q] + 1, k, cand, ncand,
-             thresh);
+  block_best(SlotKey{qv.tables + qv.table_off[q], l2_policy(true, false), qv.tag, qv.tag_mask}, qv.table_mask[q] + 1,
+             k, cand, ncand, thresh);
   write_topk(cand, q, k, out_ids, out_counts);
 }
 
@@ -383,7 +401,8 @@ __global__ void __launch_bounds__(kTopkThreads)
   const uint32_t cap = qv.table_mask[q] + 1;
   const uint32_t first = (uint32_t)(g - seg_first[q]) * seg_slots;
   const uint32_t n = cap - first < seg_slots ? cap - first : seg_slots;
-  block_best(SlotKey{qv.tables + qv.table_off[q] + first, l2_policy(true, false)}, n, k, cand, ncand, thresh);
+  block_best(SlotKey{qv.tables + qv.table_off[q] + first, l2_policy(true, false), qv.tag, qv.tag_mask}, n, k, cand,
+             ncand, thresh);
   if (nseg == 1) {
     write_topk(cand, q, k, out_ids, out_counts);
   } else {
@@ -462,7 +481,7 @@ cudaError_t launch_clear_tables(unsigned long long* tables, unsigned long long n
   if (n == 0) return cudaSuccess;
   if ((reinterpret_cast<uintptr_t>(tables) & 15) || (n & 1))  // not in 16-byte pairs: byte fill
     return cudaMemsetAsync(tables, 0xff, n * sizeof(unsigned long long), stream);
-  const unsigned long long n2 = n / 2, need = (n2 + 255) / 256, full = (unsigned long long)sm_count() * 8;
+  const unsigned long long n2 = n / 2, need = (n2 + 255) / 256, full = (unsigned long long)sm_count() * 32;
   clear_tables_kernel<<<(unsigned)(need < full ? need : full), 256, 0, stream>>>(
       reinterpret_cast<ulonglong2*>(tables), n2);
   return cudaGetLastError();

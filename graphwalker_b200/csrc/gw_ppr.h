@@ -25,13 +25,19 @@ struct QueryView {
   const unsigned long long* id_base;       // nq: stream id of query q's first walk (NULL = prefix)
   const unsigned long long* table_off;     // nq: first slot of query q's table
   const uint32_t* table_mask;              // nq: table size - 1 (power of two)
-  unsigned long long* tables;              // all tables, slots (vertex << 32 | count), ~0 = empty
+  unsigned long long* tables;              // all tables, slots ((tag | vertex) << 32 | count), ~0 = empty
   uint32_t* full;                          // nq: set to 1 when query q's table filled up
   const uint32_t* stream;                  // nq: Philox stream word of query q (NULL = 0)
   unsigned long long* visits;              // total visits counter (may be NULL)
   unsigned long long* cursor;              // batch positions handed out (zeroed by the launcher)
   uint32_t chunk;                          // walks per cursor grab (0 = kWarpChunk)
   uint32_t nq;
+  // Batch tag: the high bits of a slot's vertex word (tag_mask) hold the tag
+  // of the batch that wrote it.  A slot whose tag is not this batch's is free,
+  // so a new tag frees every table at once without a clear.  tag_mask = 0:
+  // untagged, only ~0 is free.
+  uint32_t tag;
+  uint32_t tag_mask;
 };
 
 // Walks [w_begin, w_end) of the batch; threads_per_sm <= 0 = full occupancy.

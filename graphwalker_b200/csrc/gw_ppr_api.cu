@@ -1,12 +1,20 @@
 // gw_ppr_api.cu -- C ABI of the multi-source PPR queries (gw_ppr_run,
 // gw_ppr_autotune); the kernels are in gw_ppr.cu.
 //
+// The context's tables are not cleared between batches: each batch writes
+// its slots under a new tag (QueryView::tag), which frees the slots of every
+// earlier batch at once.  They are cleared when first allocated, when they
+// grow, and when the tags run out (2^(32 - vertex id bits) - 1 of them: 63 at
+// R-MAT scale 26).  GW_PPR_TAG_BITS caps the tag width (0 = untagged, every
+// batch cleared), so that tests reach the wrap-around on small graphs.
+//
 // Tables are sized for the typical query (table_factor slots per walk of the
 // budget).  A query whose table fills up is flagged by the kernel and run
 // again, alone with the other flagged queries, with tables four times larger:
 // its walks keep their stream ids, so the retried result is exactly the one a
 // large enough table would have given.
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 #include "gw_ctx.h"
@@ -31,6 +39,8 @@ struct QuerySet {
   std::vector<unsigned long long> seg_first;  // top-k segments per query (prefix)
   uint32_t seg_slots = gw::kTopkSegment;
   uint64_t walks = 0, slots = 0;
+  bool shared = false;        // the context's buffers (tagged), or this set's own (cleared, untagged)
+  bool fresh_tables = false;  // d_tables was (re)allocated by upload_set: its content is undefined
   gw_devbuf own[12];
   gw_devbuf *d_sources, *d_prefix, *d_id_base, *d_toff, *d_tmask, *d_tables, *d_full, *d_ids, *d_cnt, *d_cursor,
       *d_segs, *d_cand;
@@ -43,6 +53,7 @@ struct QuerySet {
     gw_devbuf** d[12] = {&d_sources, &d_prefix, &d_id_base, &d_toff, &d_tmask, &d_tables,
                          &d_full,    &d_ids,    &d_cnt,     &d_cursor, &d_segs, &d_cand};
     for (int i = 0; i < 12; ++i) *d[i] = use_ctx_buffers ? b[i] : &own[i];
+    shared = use_ctx_buffers;
   }
   ~QuerySet() {
     for (auto& b : own) b.release();
@@ -82,7 +93,10 @@ gw_status upload_set(gw_ctx* ctx, QuerySet* s, uint32_t k, cudaStream_t st) {
   GW_CUDA(ctx, s->d_id_base->ensure(n * 8), "query alloc");
   GW_CUDA(ctx, s->d_toff->ensure(n * 8), "query alloc");
   GW_CUDA(ctx, s->d_tmask->ensure(n * 4), "query alloc");
+  const void* tables0 = s->d_tables->p;
+  const size_t table_bytes0 = s->d_tables->bytes;
   GW_CUDA(ctx, s->d_tables->ensure(s->slots * 8), "query tables alloc");
+  s->fresh_tables = s->d_tables->p != tables0 || s->d_tables->bytes != table_bytes0;
   GW_CUDA(ctx, s->d_full->ensure(n * 4), "query alloc");
   GW_CUDA(ctx, s->d_ids->ensure((uint64_t)n * k * 4), "top-k alloc");
   GW_CUDA(ctx, s->d_cnt->ensure((uint64_t)n * k * 4), "top-k alloc");
@@ -111,21 +125,54 @@ gw_status upload_set(gw_ctx* ctx, QuerySet* s, uint32_t k, cudaStream_t st) {
   return GW_OK;
 }
 
+// Makes the set's tables free for a new batch: the next tag of the context's
+// tables (cleared only when they are fresh or the tags have run out), or a
+// clear of the set's own tables.  *cleared: a clear was launched.
+cudaError_t assign_tag(gw_ctx* ctx, QuerySet* s, cudaStream_t st, bool* cleared) {
+  *cleared = true;
+  const uint32_t top = ctx->nv > 1 ? ctx->nv - 1 : 1;
+  const uint32_t vbits = 32 - (uint32_t)__builtin_clz(top);  // bits of the largest vertex id
+  uint32_t tbits = 32 - vbits;
+  if (const char* cap = getenv("GW_PPR_TAG_BITS")) tbits = std::min<uint32_t>(tbits, (uint32_t)atoi(cap));
+  const uint32_t ntags = tbits >= 2 ? (1u << tbits) - 1 : 0;  // the all-ones tag is the empty pattern's
+  if (!s->shared || ntags == 0) {
+    s->qv.tag = s->qv.tag_mask = 0;
+    if (s->shared) ctx->q_tags_ok = false;  // untagged slots look like tag 0
+    return gw::launch_clear_tables(s->qv.tables, s->slots, st);
+  }
+  cudaError_t e = cudaSuccess;
+  if (s->fresh_tables || !ctx->q_tags_ok || ctx->q_tag_next >= ntags) {
+    ctx->q_tags_ok = false;
+    e = gw::launch_clear_tables(s->qv.tables, s->d_tables->bytes / 8, st);
+    if (e != cudaSuccess) return e;
+    ctx->q_tags_ok = true;
+    ctx->q_tag_next = 0;
+    s->fresh_tables = false;
+  } else {
+    *cleared = false;
+  }
+  s->qv.tag_mask = ~0u << vbits;
+  s->qv.tag = ctx->q_tag_next++ << vbits;
+  return e;
+}
+
 float elapsed(cudaEvent_t a, cudaEvent_t b) {
   float ms = 0.f;
   cudaEventElapsedTime(&ms, a, b);
   return ms;
 }
 
-// Clear + walk + top-k of a whole set in three launches (batched) or query by
-// query (plain).  Timing events: ev[0] start, ev[1] cleared, ev[2] walked, ev[3] done.
+// Tag (or clear) + walk + top-k of a whole set in two to four launches
+// (batched), or clear + walk + top-k query by query (plain).  Timing events:
+// ev[0] start, ev[1] tables free, ev[2] walked, ev[3] done.
 cudaError_t run_set(gw_ctx* ctx, const gw_walk_params* p, const gw::WalkArgs& a, QuerySet* s, uint32_t k,
                     bool batched, int threads_per_sm, cudaStream_t st, cudaEvent_t* ev, uint32_t* launches) {
   cudaError_t e = cudaSuccess;
   const uint32_t n = s->qv.nq;
   cudaEventRecord(ev[0], st);
+  bool cleared = false;
+  e = assign_tag(ctx, s, st, &cleared);
   if (batched) {
-    e = gw::launch_clear_tables(s->qv.tables, s->slots, st);
     cudaEventRecord(ev[1], st);
     if (e == cudaSuccess)
       e = gw::launch_walk_queries((int)p->rule, s->qv, 0, s->walks, ctx->view(), a, ctx->d_status.as<uint32_t>(),
@@ -136,9 +183,10 @@ cudaError_t run_set(gw_ctx* ctx, const gw_walk_params* p, const gw::WalkArgs& a,
                                     s->d_segs->as<unsigned long long>(), s->seg_first.data(), s->seg_slots,
                                     s->d_cand->as<unsigned long long>(), st);
     cudaEventRecord(ev[3], st);
-    *launches += s->seg_first[n] > n ? 4 : 3;
+    *launches += (s->seg_first[n] > n ? 3 : 2) + (cleared ? 1 : 0);
   } else {
     cudaEventRecord(ev[1], st);
+    *launches += cleared ? 1 : 0;
     for (uint32_t q = 0; q < n && e == cudaSuccess; ++q) {
       e = gw::launch_clear_tables(s->qv.tables + s->toff[q], (uint64_t)s->tmask[q] + 1, st);
       if (e == cudaSuccess)
@@ -275,7 +323,8 @@ extern "C" gw_status gw_ppr_autotune(gw_ctx* ctx, const gw_walk_params* params, 
       set.qv.chunk = ch;
       float ms_sum = 0.f;
       for (int rep = 0; rep < 3; ++rep) {
-        gw::launch_clear_tables(set.qv.tables, set.slots, st);
+        bool cleared = false;
+        if (assign_tag(ctx, &set, st, &cleared) != cudaSuccess) break;
         cudaEventRecord(e0, st);
         gw::launch_walk_queries((int)params->rule, set.qv, 0, set.walks, ctx->view(), a,
                                 ctx->d_status.as<uint32_t>(), c, st);

@@ -62,6 +62,30 @@ def test_ppr_queries_match_oracle(cuda_device, oracle, rule, L, layout):
             assert st.walks == budgets.sum()
 
 
+@pytest.mark.parametrize("tag_bits", [None, "2", "0"], ids=["tags", "3_tags", "untagged"])
+def test_batches_reuse_tables_exactly(cuda_device, oracle, monkeypatch, tag_bits):
+    """Consecutive batches in one context, with different table layouts
+    (growing, shrinking): each batch writes under a new tag and sees none of
+    the earlier batches' slots.  With 3 tags the tables are cleared every
+    third batch; untagged, every batch.  Each result equals the oracle's."""
+    import graphwalker_b200 as gw
+    if tag_bits is None:
+        monkeypatch.delenv("GW_PPR_TAG_BITS", raising=False)
+    else:
+        monkeypatch.setenv("GW_PPR_TAG_BITS", tag_bits)
+    rp, ci = oracle.rmat_csr(12, 8, seed=5)
+    deg = np.diff(rp.astype(np.int64))
+    rng = np.random.default_rng(31)
+    p = gw.params(gw.RULE_STOP, gw.SINK_NONE, 20, seed=8)
+    with gw.Graph.from_csr(rp, ci, oracle.compute_blocks(rp, 64)) as G:
+        for nq, top in [(20, 300), (30, 1200), (10, 50), (40, 900), (25, 2500), (5, 20), (30, 600), (15, 1500)]:
+            sources = rng.choice(np.nonzero(deg)[0], nq).astype(np.uint32)
+            budgets = rng.integers(1, top, nq).astype(np.uint32)
+            ref_ids, ref_cnt = _oracle_queries(oracle, rp, ci, sources, budgets, 1, 20, 8, 30)
+            ids, cnt, _ = G.ppr(p, sources, budgets, k=30)
+            assert np.array_equal(ids, ref_ids) and np.array_equal(cnt, ref_cnt), (nq, top)
+
+
 def test_ppr_batched_equals_plain_at_scale(cuda_device):
     import graphwalker_b200 as gw
     with gw.Graph.rmat(18, 16, seed=4, blocksize_kb=1024) as G:
