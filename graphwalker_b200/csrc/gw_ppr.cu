@@ -306,6 +306,11 @@ __device__ void block_best(Src src, uint32_t n, uint32_t k, unsigned long long* 
     thresh = 0;
   }
   __syncthreads();
+  // nc: the candidate count, kept in a register by every thread alike.  The
+  // shared ncand only hands out positions: a thread that already appends in
+  // the next step changes it while slower threads would still be reading it
+  // for the cut decision, so that decision must not read it.
+  uint32_t nc = 0;
   for (uint32_t base = 0; base < n; base += blockDim.x * kTopkUnroll) {
     unsigned long long raw[kTopkUnroll];
 #pragma unroll
@@ -316,23 +321,22 @@ __device__ void block_best(Src src, uint32_t n, uint32_t k, unsigned long long* 
 #pragma unroll
     for (uint32_t u = 0; u < kTopkUnroll; ++u) {
       const unsigned long long key = src.key(raw[u]);
-      if (key > thresh) {
-        const uint32_t pos = atomicAdd(&ncand, 1u);
-        cand[pos] = key;  // room for one full round is kept free below
-      }
-      __syncthreads();
-      if (ncand > kTopkBuffer - blockDim.x) {  // cut to the best k before the next round
-        for (uint32_t x = ncand + threadIdx.x; x < kTopkBuffer; x += blockDim.x) cand[x] = 0;
+      const bool take = key > thresh;
+      if (take) cand[atomicAdd(&ncand, 1u)] = key;  // room for one full step is kept free below
+      nc += (uint32_t)__syncthreads_count(take);
+      if (nc > kTopkBuffer - blockDim.x) {  // cut to the best k before the next step
+        for (uint32_t x = nc + threadIdx.x; x < kTopkBuffer; x += blockDim.x) cand[x] = 0;
         block_sort_desc(cand, kTopkBuffer);
         if (threadIdx.x == 0) {
           ncand = k;
           thresh = cand[k - 1];
         }
+        nc = k;
         __syncthreads();
       }
     }
   }
-  for (uint32_t x = ncand + threadIdx.x; x < kTopkBuffer; x += blockDim.x) cand[x] = 0;
+  for (uint32_t x = nc + threadIdx.x; x < kTopkBuffer; x += blockDim.x) cand[x] = 0;
   block_sort_desc(cand, kTopkBuffer);
 }
 
@@ -366,30 +370,33 @@ __device__ void write_topk(const unsigned long long* cand, uint32_t q, uint32_t 
   }
 }
 
-// One CTA per query over its whole table.
+// One CTA per query over its whole table; CTA i takes query q_begin +
+// order[i] (order NULL: i).
 __global__ void __launch_bounds__(kTopkThreads)
-    topk_kernel(QueryView qv, uint32_t q_begin, uint32_t k, uint32_t* __restrict__ out_ids,
-                uint32_t* __restrict__ out_counts) {
+    topk_kernel(QueryView qv, uint32_t q_begin, uint32_t k, const uint32_t* __restrict__ order,
+                uint32_t* __restrict__ out_ids, uint32_t* __restrict__ out_counts) {
   __shared__ unsigned long long cand[kTopkBuffer];
   __shared__ uint32_t ncand;
   __shared__ unsigned long long thresh;
-  const uint32_t q = q_begin + blockIdx.x;
+  const uint32_t q = q_begin + (order ? __ldg(order + blockIdx.x) : blockIdx.x);
   block_best(SlotKey{qv.tables + qv.table_off[q], l2_policy(true, false), qv.tag, qv.tag_mask}, qv.table_mask[q] + 1,
              k, cand, ncand, thresh);
   write_topk(cand, q, k, out_ids, out_counts);
 }
 
-// One CTA per table segment of seg_slots slots: a query with one segment
+// One CTA per table segment of seg_slots slots (CTA i takes segment
+// seg_first[q_begin] + order[i]; order NULL: i): a query with one segment
 // gets its list here; the others leave their segments' best k keys in
 // seg_cand for topk_merge_kernel.
 __global__ void __launch_bounds__(kTopkThreads)
     topk_segment_kernel(QueryView qv, uint32_t q_begin, uint32_t q_count, uint32_t k, uint32_t seg_slots,
-                        const unsigned long long* __restrict__ seg_first, unsigned long long* __restrict__ seg_cand,
-                        uint32_t* __restrict__ out_ids, uint32_t* __restrict__ out_counts) {
+                        const unsigned long long* __restrict__ seg_first, const uint32_t* __restrict__ order,
+                        unsigned long long* __restrict__ seg_cand, uint32_t* __restrict__ out_ids,
+                        uint32_t* __restrict__ out_counts) {
   __shared__ unsigned long long cand[kTopkBuffer];
   __shared__ uint32_t ncand;
   __shared__ unsigned long long thresh;
-  const unsigned long long g = seg_first[q_begin] + blockIdx.x;
+  const unsigned long long g = seg_first[q_begin] + (order ? __ldg(order + blockIdx.x) : blockIdx.x);
   uint32_t lo = q_begin, hi = q_begin + q_count - 1;  // the query holding segment g
   while (lo < hi) {
     const uint32_t mid = (lo + hi + 1) >> 1;
@@ -499,20 +506,38 @@ void topk_segment_prefix(const uint32_t* table_mask, uint32_t nq, uint32_t seg_s
     seg_first[q + 1] = seg_first[q] + ((unsigned long long)table_mask[q] + seg_slots) / seg_slots;
 }
 
+void topk_segment_order(const uint32_t* table_mask, uint32_t nq, uint32_t seg_slots,
+                        const unsigned long long* seg_first, uint32_t* order) {
+  // a table is a power of two, so is a segment: bucket the segments by
+  // log2(size), largest bucket first, each bucket in segment order
+  std::vector<uint32_t> start(34, 0);
+  auto bucket = [&](uint32_t q, unsigned long long i) {
+    const unsigned long long cap = (unsigned long long)table_mask[q] + 1, first = i * seg_slots;
+    const unsigned long long size = cap - first < seg_slots ? cap - first : seg_slots;
+    return 63 - __builtin_clzll(size);  // 0..32
+  };
+  for (uint32_t q = 0; q < nq; ++q)
+    for (unsigned long long i = 0; i < seg_first[q + 1] - seg_first[q]; ++i) ++start[32 - bucket(q, i) + 1];
+  for (int b = 1; b < 34; ++b) start[b] += start[b - 1];
+  for (uint32_t q = 0; q < nq; ++q)
+    for (unsigned long long i = 0; i < seg_first[q + 1] - seg_first[q]; ++i)
+      order[start[32 - bucket(q, i)]++] = (uint32_t)(seg_first[q] + i);
+}
+
 cudaError_t launch_topk_segmented(const QueryView& qv, uint32_t q_begin, uint32_t q_count, uint32_t k,
                                   uint32_t* out_ids, uint32_t* out_counts, const unsigned long long* d_seg_first,
                                   const unsigned long long* h_seg_first, uint32_t seg_slots,
-                                  unsigned long long* d_seg_cand, cudaStream_t stream) {
+                                  unsigned long long* d_seg_cand, const uint32_t* d_order, cudaStream_t stream) {
   if (q_count == 0) return cudaSuccess;
   if (k == 0 || k > kTopkMaxK) return cudaErrorInvalidValue;
   const unsigned long long nseg = h_seg_first[q_begin + q_count] - h_seg_first[q_begin];
   if (nseg == 0 || nseg > 0x7fffffffull) return cudaErrorInvalidValue;
   if (nseg == q_count) {  // no table is split: one CTA per query
-    topk_kernel<<<q_count, kTopkThreads, 0, stream>>>(qv, q_begin, k, out_ids, out_counts);
+    topk_kernel<<<q_count, kTopkThreads, 0, stream>>>(qv, q_begin, k, d_order, out_ids, out_counts);
     return cudaGetLastError();
   }
   topk_segment_kernel<<<(unsigned)nseg, kTopkThreads, 0, stream>>>(qv, q_begin, q_count, k, seg_slots, d_seg_first,
-                                                                    d_seg_cand, out_ids, out_counts);
+                                                                    d_order, d_seg_cand, out_ids, out_counts);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess && nseg > q_count) {  // some query has several segments
     topk_merge_kernel<<<q_count, kTopkThreads, 0, stream>>>(q_begin, k, d_seg_first, d_seg_cand, out_ids, out_counts);
@@ -525,7 +550,7 @@ cudaError_t launch_topk(const QueryView& qv, uint32_t q_begin, uint32_t q_count,
                         uint32_t* out_counts, cudaStream_t stream) {
   if (q_count == 0) return cudaSuccess;
   if (k == 0 || k > kTopkMaxK) return cudaErrorInvalidValue;
-  topk_kernel<<<q_count, kTopkThreads, 0, stream>>>(qv, q_begin, k, out_ids, out_counts);
+  topk_kernel<<<q_count, kTopkThreads, 0, stream>>>(qv, q_begin, k, nullptr, out_ids, out_counts);
   return cudaGetLastError();
 }
 

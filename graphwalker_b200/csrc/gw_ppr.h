@@ -56,10 +56,17 @@ void topk_segment_prefix(const uint32_t* table_mask, uint32_t nq, uint32_t seg_s
 // Top-k of queries [q_begin, q_begin + q_count) into out[q * k + r], one CTA
 // per kTopkSegment slots of table: seg_first (nq + 1, on the device and the
 // host) from topk_segment_prefix, seg_cand k keys of scratch per segment.
+// d_order (NULL = segment order): the launch order of the segments, from
+// topk_segment_order, as offsets from seg_first[q_begin].
 cudaError_t launch_topk_segmented(const QueryView& qv, uint32_t q_begin, uint32_t q_count, uint32_t k,
                                   uint32_t* out_ids, uint32_t* out_counts, const unsigned long long* d_seg_first,
                                   const unsigned long long* h_seg_first, uint32_t seg_slots,
-                                  unsigned long long* d_seg_cand, cudaStream_t stream);
+                                  unsigned long long* d_seg_cand, const uint32_t* d_order, cudaStream_t stream);
+// The segments of all nq queries (seg_first[nq] of them), largest first (host):
+// a CTA ranking a large table starts in the first wave instead of after the
+// small ones, where it would run alone at the end of the launch.
+void topk_segment_order(const uint32_t* table_mask, uint32_t nq, uint32_t seg_slots,
+                        const unsigned long long* seg_first, uint32_t* order);
 // Top-k of queries [q_begin, q_begin + q_count) into out[q * k + r], one CTA per query.
 cudaError_t launch_topk(const QueryView& qv, uint32_t q_begin, uint32_t q_count, uint32_t k, uint32_t* out_ids,
                         uint32_t* out_counts, cudaStream_t stream);

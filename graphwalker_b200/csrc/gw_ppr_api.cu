@@ -37,6 +37,7 @@ struct QuerySet {
   std::vector<unsigned long long> prefix, id_base, toff;
   std::vector<uint32_t> tmask;
   std::vector<unsigned long long> seg_first;  // top-k segments per query (prefix)
+  std::vector<uint32_t> seg_order;            // top-k segments in launch order, largest first
   uint32_t seg_slots = gw::kTopkSegment;
   uint64_t walks = 0, slots = 0;
   bool shared = false;        // the context's buffers (tagged), or this set's own (cleared, untagged)
@@ -104,9 +105,14 @@ gw_status upload_set(gw_ctx* ctx, QuerySet* s, uint32_t k, cudaStream_t st) {
   s->seg_first.resize(n + 1);
   s->seg_slots = gw::topk_segment_slots(n);
   gw::topk_segment_prefix(s->tmask.data(), n, s->seg_slots, s->seg_first.data());
-  GW_CUDA(ctx, s->d_segs->ensure((n + 1) * 8), "top-k segments");
+  s->seg_order.resize(s->seg_first[n]);
+  gw::topk_segment_order(s->tmask.data(), n, s->seg_slots, s->seg_first.data(), s->seg_order.data());
+  // d_segs: seg_first (n + 1 u64), then seg_order (u32 per segment)
+  GW_CUDA(ctx, s->d_segs->ensure((n + 1) * 8 + s->seg_first[n] * 4), "top-k segments");
   GW_CUDA(ctx, s->d_cand->ensure(s->seg_first[n] * k * 8 + 8), "top-k candidates");
   GW_CUDA(ctx, cudaMemcpyAsync(s->d_segs->p, s->seg_first.data(), (n + 1) * 8, cudaMemcpyHostToDevice, st), "copy");
+  GW_CUDA(ctx, cudaMemcpyAsync(s->d_segs->as<unsigned long long>() + n + 1, s->seg_order.data(), s->seg_first[n] * 4,
+                               cudaMemcpyHostToDevice, st), "copy");
   GW_CUDA(ctx, cudaMemcpyAsync(s->d_sources->p, s->sources.data(), n * 4, cudaMemcpyHostToDevice, st), "copy");
   GW_CUDA(ctx, cudaMemcpyAsync(s->d_prefix->p, s->prefix.data(), (n + 1) * 8, cudaMemcpyHostToDevice, st), "copy");
   GW_CUDA(ctx, cudaMemcpyAsync(s->d_id_base->p, s->id_base.data(), n * 8, cudaMemcpyHostToDevice, st), "copy");
@@ -181,7 +187,8 @@ cudaError_t run_set(gw_ctx* ctx, const gw_walk_params* p, const gw::WalkArgs& a,
     if (e == cudaSuccess)
       e = gw::launch_topk_segmented(s->qv, 0, n, k, s->d_ids->as<uint32_t>(), s->d_cnt->as<uint32_t>(),
                                     s->d_segs->as<unsigned long long>(), s->seg_first.data(), s->seg_slots,
-                                    s->d_cand->as<unsigned long long>(), st);
+                                    s->d_cand->as<unsigned long long>(),
+                                    reinterpret_cast<const uint32_t*>(s->d_segs->as<unsigned long long>() + n + 1), st);
     cudaEventRecord(ev[3], st);
     *launches += (s->seg_first[n] > n ? 3 : 2) + (cleared ? 1 : 0);
   } else {
@@ -195,7 +202,7 @@ cudaError_t run_set(gw_ctx* ctx, const gw_walk_params* p, const gw::WalkArgs& a,
       if (e == cudaSuccess)
         e = gw::launch_topk_segmented(s->qv, q, 1, k, s->d_ids->as<uint32_t>(), s->d_cnt->as<uint32_t>(),
                                       s->d_segs->as<unsigned long long>(), s->seg_first.data(), s->seg_slots,
-                                      s->d_cand->as<unsigned long long>(), st);
+                                      s->d_cand->as<unsigned long long>(), nullptr, st);
       *launches += s->seg_first[q + 1] - s->seg_first[q] > 1 ? 1 : 0;
     }
     cudaEventRecord(ev[2], st);

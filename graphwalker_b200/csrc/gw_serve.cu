@@ -290,7 +290,7 @@ bool superstep(gw_server* srv) {
         e = cudaMemcpyAsync(srv->d_topk_segs.p, sf.data(), (nfin + 1) * 8, cudaMemcpyHostToDevice, st);
       if (e == cudaSuccess)
         e = gw::launch_topk_segmented(qv, 0, nfin, k, d.ids, d.counts, srv->d_topk_segs.as<unsigned long long>(),
-                                      sf.data(), seg_slots, srv->d_topk_cand.as<unsigned long long>(), st);
+                                      sf.data(), seg_slots, srv->d_topk_cand.as<unsigned long long>(), nullptr, st);
       if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // sf is read by the copy above
     }
   }

@@ -86,6 +86,25 @@ def test_batches_reuse_tables_exactly(cuda_device, oracle, monkeypatch, tag_bits
             assert np.array_equal(ids, ref_ids) and np.array_equal(cnt, ref_cnt), (nq, top)
 
 
+def test_split_tables_ranked_largest_first_match_oracle(cuda_device, oracle):
+    """Tables of 2 to 8 top-k segments beside one-segment tables: the
+    segments are ranked largest first and merged per query; each list equals
+    the oracle's."""
+    import graphwalker_b200 as gw
+    rp, ci = oracle.rmat_csr(12, 8, seed=6)
+    deg = np.diff(rp.astype(np.int64))
+    rng = np.random.default_rng(4)
+    budgets = np.array([5000, 20, 3000, 1, 70, 9000, 400, 2500], np.uint32)
+    sources = rng.choice(np.nonzero(deg)[0], len(budgets)).astype(np.uint32)
+    ref_ids, ref_cnt = _oracle_queries(oracle, rp, ci, sources, budgets, 1, 20, 3, 100)
+    p = gw.params(gw.RULE_STOP, gw.SINK_NONE, 20, seed=3)
+    with gw.Graph.from_csr(rp, ci, oracle.compute_blocks(rp, 64)) as G:
+        for batched in (True, False):
+            ids, cnt, st = G.ppr(p, sources, budgets, k=100, batched=batched)
+            assert np.array_equal(ids, ref_ids) and np.array_equal(cnt, ref_cnt), f"batched={batched}"
+        assert st.table_slots > 16384 * len(budgets)  # some tables span several segments
+
+
 def test_ppr_batched_equals_plain_at_scale(cuda_device):
     import graphwalker_b200 as gw
     with gw.Graph.rmat(18, 16, seed=4, blocksize_kb=1024) as G:
@@ -101,6 +120,9 @@ def test_ppr_batched_equals_plain_at_scale(cuda_device):
         assert np.array_equal(ib, ip) and np.array_equal(cb, cp)
         # the source is visited by every walk at hop 0
         assert np.all(cb[:, 0] >= budgets)
+        for _ in range(3):  # repeated batches: the same lists every time
+            ir, cr, _ = G.ppr(p, sources, budgets, k=100, batched=True)
+            assert np.array_equal(ir, ip) and np.array_equal(cr, cp)
         threads, chunk = G.ppr_autotune(p, sources[:50], budgets[:50])
         assert threads in (512, 1024, 1536, 2048) and chunk in (64, 128, 256, 512)
         it, ct, _ = G.ppr(p, sources, budgets, k=100, batched=True)
