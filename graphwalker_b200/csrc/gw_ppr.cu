@@ -291,13 +291,97 @@ __device__ void block_sort_desc(unsigned long long* keys, uint32_t n) {
   __syncthreads();
 }
 
+// Cuts cand[0, nc) (distinct nonzero keys, nc > k) to its k largest, in any
+// order, at cand[0, *kept), and returns the smallest of them.  The k-th
+// largest key is found by an MSB-first radix select on 8-bit digits (a
+// histogram of the keys that match the digits chosen so far, one warp picks
+// the digit holding rank k), which stops early once the wanted key is the
+// smallest of its bucket; one compaction pass then keeps the keys >= it.
+// Costs about 3 barriers per digit, where a bitonic sort of the buffer
+// takes 55.
+__device__ unsigned long long cut_to_k(unsigned long long* cand, uint32_t nc, uint32_t k, uint32_t* kept_out) {
+  __shared__ uint32_t hist[256];
+  __shared__ uint32_t sel[3];  // chosen digit, rank left inside it, keys in its bucket
+  __shared__ unsigned long long kth;
+  __shared__ uint32_t kept;
+  const uint32_t lane = threadIdx.x & 31;
+  unsigned long long prefix = 0, pmask = 0;
+  uint32_t need = k;  // rank (1 = largest) of the wanted key among those matching prefix
+  bool smallest_of_bucket = false;
+  for (int shift = 56; shift >= 0 && !smallest_of_bucket; shift -= 8) {
+    for (uint32_t b = threadIdx.x; b < 256; b += blockDim.x) hist[b] = 0;
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < nc; x += blockDim.x) {
+      const unsigned long long key = cand[x];
+      if ((key & pmask) == prefix) atomicAdd(&hist[(uint32_t)(key >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {  // lane l holds bins 255 - 8l down to 248 - 8l
+      uint32_t sum = 0;
+      for (uint32_t i = 0; i < 8; ++i) sum += hist[255 - 8 * lane - i];
+      uint32_t incl = sum;  // keys in the bins of lanes 0..l
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(~0u, incl, o);
+        if (lane >= (uint32_t)o) incl += y;
+      }
+      const uint32_t above = incl - sum;
+      if (above < need && need <= incl) {
+        uint32_t c = above;
+        for (uint32_t i = 0; i < 8; ++i) {
+          const uint32_t h = hist[255 - 8 * lane - i];
+          if (c + h >= need) {
+            sel[0] = 255 - 8 * lane - i;
+            sel[1] = need - c;
+            sel[2] = h;
+            break;
+          }
+          c += h;
+        }
+      }
+    }
+    __syncthreads();
+    prefix |= (unsigned long long)sel[0] << shift;
+    pmask |= 255ull << shift;
+    need = sel[1];
+    smallest_of_bucket = sel[2] == need;
+    __syncthreads();  // sel and hist are rewritten by the next digit
+  }
+  if (threadIdx.x == 0) {
+    kth = smallest_of_bucket ? ~0ull : prefix;
+    kept = 0;
+  }
+  __syncthreads();
+  if (smallest_of_bucket) {
+    for (uint32_t x = threadIdx.x; x < nc; x += blockDim.x) {
+      const unsigned long long key = cand[x];
+      if ((key & pmask) == prefix) atomicMin(&kth, key);
+    }
+    __syncthreads();
+  }
+  const unsigned long long t = kth;
+  unsigned long long mine[kTopkBuffer / kTopkThreads];
+#pragma unroll
+  for (uint32_t i = 0; i < kTopkBuffer / kTopkThreads; ++i) {
+    const uint32_t x = threadIdx.x + i * blockDim.x;
+    mine[i] = x < nc ? cand[x] : 0ull;
+  }
+  __syncthreads();
+#pragma unroll
+  for (uint32_t i = 0; i < kTopkBuffer / kTopkThreads; ++i)
+    if (mine[i] != 0ull && mine[i] >= t) cand[atomicAdd(&kept, 1u)] = mine[i];
+  __syncthreads();
+  *kept_out = kept;
+  return t;
+}
+
 // The best k keys of n (key i = src.key(src.fetch(i)); 0 = no key) into
 // cand[0, k), largest first.  kTopkUnroll values per thread are fetched
 // before any is converted (the loads issue back to back, so a large table is
-// read with that many loads in flight per thread), then filtered one round of
+// read with that many loads in flight per thread), then filtered one step of
 // blockDim.x keys at a time into the candidate buffer; whenever the buffer
-// could overflow it is sorted and cut to the best k, and the k-th key becomes
-// the admission threshold.
+// could overflow it is cut to the best k (cut_to_k), and the k-th key
+// becomes the admission threshold.  Only the final k are sorted.
 template <typename Src>
 __device__ void block_best(Src src, uint32_t n, uint32_t k, unsigned long long* cand, uint32_t& ncand,
                            unsigned long long& thresh) {
@@ -325,19 +409,26 @@ __device__ void block_best(Src src, uint32_t n, uint32_t k, unsigned long long* 
       if (take) cand[atomicAdd(&ncand, 1u)] = key;  // room for one full step is kept free below
       nc += (uint32_t)__syncthreads_count(take);
       if (nc > kTopkBuffer - blockDim.x) {  // cut to the best k before the next step
-        for (uint32_t x = nc + threadIdx.x; x < kTopkBuffer; x += blockDim.x) cand[x] = 0;
-        block_sort_desc(cand, kTopkBuffer);
+        uint32_t kept = 0;
+        const unsigned long long t = cut_to_k(cand, nc, k, &kept);
         if (threadIdx.x == 0) {
-          ncand = k;
-          thresh = cand[k - 1];
+          ncand = kept;
+          thresh = t;
         }
-        nc = k;
+        nc = kept;
         __syncthreads();
       }
     }
   }
-  for (uint32_t x = nc + threadIdx.x; x < kTopkBuffer; x += blockDim.x) cand[x] = 0;
-  block_sort_desc(cand, kTopkBuffer);
+  if (nc > k) {
+    uint32_t kept = 0;
+    cut_to_k(cand, nc, k, &kept);
+    nc = kept;
+  }
+  uint32_t m = 1;
+  while (m < k) m <<= 1;
+  for (uint32_t x = nc + threadIdx.x; x < m; x += blockDim.x) cand[x] = 0;
+  block_sort_desc(cand, m);
 }
 
 // Key of a table slot: count << 32 | ~vertex (larger = more visits, then the
@@ -372,7 +463,7 @@ __device__ void write_topk(const unsigned long long* cand, uint32_t q, uint32_t 
 
 // One CTA per query over its whole table; CTA i takes query q_begin +
 // order[i] (order NULL: i).
-__global__ void __launch_bounds__(kTopkThreads)
+__global__ void __launch_bounds__(kTopkThreads, 3)
     topk_kernel(QueryView qv, uint32_t q_begin, uint32_t k, const uint32_t* __restrict__ order,
                 uint32_t* __restrict__ out_ids, uint32_t* __restrict__ out_counts) {
   __shared__ unsigned long long cand[kTopkBuffer];
@@ -388,7 +479,7 @@ __global__ void __launch_bounds__(kTopkThreads)
 // seg_first[q_begin] + order[i]; order NULL: i): a query with one segment
 // gets its list here; the others leave their segments' best k keys in
 // seg_cand for topk_merge_kernel.
-__global__ void __launch_bounds__(kTopkThreads)
+__global__ void __launch_bounds__(kTopkThreads, 3)
     topk_segment_kernel(QueryView qv, uint32_t q_begin, uint32_t q_count, uint32_t k, uint32_t seg_slots,
                         const unsigned long long* __restrict__ seg_first, const uint32_t* __restrict__ order,
                         unsigned long long* __restrict__ seg_cand, uint32_t* __restrict__ out_ids,
@@ -418,7 +509,7 @@ __global__ void __launch_bounds__(kTopkThreads)
 }
 
 // One CTA per query with several segments: the best k of its segments' lists.
-__global__ void __launch_bounds__(kTopkThreads)
+__global__ void __launch_bounds__(kTopkThreads, 3)
     topk_merge_kernel(uint32_t q_begin, uint32_t k, const unsigned long long* __restrict__ seg_first,
                       const unsigned long long* __restrict__ seg_cand, uint32_t* __restrict__ out_ids,
                       uint32_t* __restrict__ out_counts) {
