@@ -661,7 +661,7 @@ def ppr1_arm(args) -> None:
                                    f"vertex), stop p=0.15, dangling->source, L<=20", "walk_steps": steps},
             "queries_per_s": 1e3 / ms,
             "ppr_api": {"device_ms": statistics.median(api_dev), "wall_ms": statistics.median(api_wall),
-                        "what": "gw_ppr_run, one query of the same walks, table clear + walk + top-100, warm"},
+                        "what": "gw_ppr_run, one query of the same walks, batch tag + walk + top-100, warm"},
             "accuracy": {"l1_error": l1, "mc_bound_l1": bound, "top100_overlap_with_fp64": overlap,
                          "top100_api_equals_counts": bool(np.array_equal(ids[0], top_from_counts))}}
     G.close()
