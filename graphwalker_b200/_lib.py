@@ -33,7 +33,8 @@ class WalkParams(Structure):
                 ("jump_prob", c_double), ("seed", c_uint64), ("mode", c_uint32),
                 ("path_stride", c_uint32), ("max_hops", c_uint32), ("prob", c_float),
                 ("aggregate", c_uint32), ("max_supersteps", c_uint32), ("cache_hints", c_uint32),
-                ("table_factor", c_uint32), ("reserved", c_uint32 * 4)]
+                ("table_factor", c_uint32), ("block_lo", c_uint32), ("block_hi", c_uint32),
+                ("reserved", c_uint32 * 2)]
 
 
 SERVE_BATCHED, SERVE_PLAIN = 0, 1

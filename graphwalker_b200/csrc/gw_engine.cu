@@ -86,6 +86,13 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     return ctx->fail(GW_E_INVALID, "PATH_RECORD needs GW_MODE_RESIDENT");
   const uint32_t nb = ctx->nblocks;
   if (nb + 1 > 8000) return ctx->fail(GW_E_INVALID, "at most 7999 blocks in blocked mode");
+  // Owned blocks (one rank of a vertex-partitioned run): only the blocks in
+  // [own_lo, own_hi) execute, and walks that move to other blocks wait in
+  // those blocks' pools for gw_read_pool.  block_hi = 0: every block.
+  const uint32_t own_lo = p->block_hi ? p->block_lo : 0, own_hi = p->block_hi ? p->block_hi : nb;
+  if (own_lo >= own_hi || own_hi > nb)
+    return ctx->fail(GW_E_INVALID, "owned blocks [%u, %u) not inside [0, %u)", p->block_lo, p->block_hi, nb);
+  const bool restricted = own_lo > 0 || own_hi < nb;
   const bool streaming = ctx->residency == GW_STREAM_PINNED;
   cudaStream_t st = ctx->stream, xs = ctx->copy_stream;
 
@@ -120,6 +127,10 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     walksum += m;
   }
   const uint64_t nwalks = walksum;
+  walksum = 0;  // from here on: walks pending in the owned blocks
+  for (uint32_t b = own_lo; b < own_hi; ++b) walksum += ctx->pool_size[b];
+  std::vector<uint64_t> own_num;
+  std::vector<uint32_t> own_min;
 
   // ---- sinks ----
   SinkView sv{};
@@ -245,7 +256,18 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
   bool pending = false;
   while (walksum > 0 && e == cudaSuccess &&
          (p->max_supersteps == 0 || superstep < p->max_supersteps)) {
-    const uint32_t b = choose_block(ctx->pool_size, ctx->minstep, p->prob, p->seed, superstep);
+    uint32_t b;
+    if (restricted) {  // the policy sees the owned blocks only
+      own_num.assign(nb, 0);
+      own_min.assign(nb, 0xffff);
+      for (uint32_t q = own_lo; q < own_hi; ++q) {
+        own_num[q] = ctx->pool_size[q];
+        own_min[q] = ctx->minstep[q];
+      }
+      b = choose_block(own_num, own_min, p->prob, p->seed, superstep);
+    } else {
+      b = choose_block(ctx->pool_size, ctx->minstep, p->prob, p->seed, superstep);
+    }
     const uint64_t n = ctx->pool_size[b];
     if (n == 0) return ctx->fail(GW_E_STATE, "scheduler chose an empty block (walksum %llu)",
                                  (unsigned long long)walksum);
@@ -355,7 +377,7 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     for (uint32_t d = 0; d < nb; ++d) {
       if (!h_totals[d]) continue;
       ctx->pool_size[d] += h_totals[d];
-      forwarded += h_totals[d];
+      if (d >= own_lo && d < own_hi) forwarded += h_totals[d];
       ctx->minstep[d] = std::min<uint32_t>(ctx->minstep[d], std::min<uint32_t>(h_minhop[d], 0xffff));
     }
     walksum = walksum - n + forwarded;

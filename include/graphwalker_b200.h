@@ -100,7 +100,13 @@ typedef struct gw_walk_params {
                            engine default; otherwise GW_HINT_EXPLICIT | bits  */
   uint32_t table_factor; /* PPR queries: table slots per walk of the budget,
                             rounded up to a power of two (0 = 8)           */
-  uint32_t reserved[4];
+  uint32_t block_lo;     /* blocked mode: only blocks [block_lo, block_hi)
+                            execute; walks that move to other blocks stay in
+                            their pools for gw_read_pool (one rank of a
+                            vertex-partitioned run).  No counterpart in the
+                            reference, whose engine runs every block.       */
+  uint32_t block_hi;     /* 0 = every block                                 */
+  uint32_t reserved[2];
 } gw_walk_params;
 
 typedef struct gw_run_stats {
