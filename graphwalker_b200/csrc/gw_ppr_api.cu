@@ -253,12 +253,20 @@ extern "C" gw_status gw_ppr_run(gw_ctx* ctx, const gw_walk_params* params, const
     const bool b = batched || round > 0;
     cudaError_t e = run_set(ctx, params, a, &set, k, b, b ? ctx->ppr_threads_per_sm : 0, st, ev, &local.launches);
     const uint32_t n = (uint32_t)which.size();
+    // The first round holds every query in the caller's order: its lists go
+    // straight into the caller's arrays (a rerun query's rows are overwritten
+    // later); a rerun's lists go through host staging to their rows.
+    const bool direct = round == 0;
     full.resize(n);
-    hid.resize((size_t)n * k);
-    hcnt.resize((size_t)n * k);
+    if (!direct) {
+      hid.resize((size_t)n * k);
+      hcnt.resize((size_t)n * k);
+    }
+    uint32_t* ids_out = direct ? topk_ids : hid.data();
+    uint32_t* cnt_out = direct ? topk_counts : hcnt.data();
     if (e == cudaSuccess) e = cudaMemcpyAsync(full.data(), set.d_full->p, n * 4, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(hid.data(), set.d_ids->p, (size_t)n * k * 4, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(hcnt.data(), set.d_cnt->p, (size_t)n * k * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ids_out, set.d_ids->p, (size_t)n * k * 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(cnt_out, set.d_cnt->p, (size_t)n * k * 4, cudaMemcpyDeviceToHost, st);
     if (e != cudaSuccess) {
       s = ctx->cuda_fail(e, "gw_ppr_run");
       break;
@@ -279,6 +287,7 @@ extern "C" gw_status gw_ppr_run(gw_ctx* ctx, const gw_walk_params* params, const
         again.push_back(q);
         continue;
       }
+      if (direct) continue;
       std::copy(hid.begin() + (size_t)i * k, hid.begin() + (size_t)(i + 1) * k, topk_ids + (size_t)q * k);
       std::copy(hcnt.begin() + (size_t)i * k, hcnt.begin() + (size_t)(i + 1) * k, topk_counts + (size_t)q * k);
     }
