@@ -52,6 +52,10 @@ class Partition:
     """One rank's share of a partitioned run on its graph context."""
 
     def __init__(self, graph, params, rank: int, world: int):
+        if params.sink != _lib.SINK_VERTEX_COUNT:
+            raise ValueError("a partitioned run counts visits per vertex (SINK_VERTEX_COUNT)")
+        if not 0 <= rank < world:
+            raise ValueError(f"rank {rank} outside a world of {world}")
         self.g = graph
         self.rank, self.world = rank, world
         self.lo, self.hi = owned_blocks(graph.nblocks, rank, world)
@@ -84,10 +88,14 @@ class Partition:
 
     def step(self) -> list[np.ndarray]:
         """Runs the owned blocks until no walk is left in them and returns the
-        walks that left, one (n, 4) array of (cur, id, src, hop) per rank."""
+        walks that left, one (n, 4) array of (cur, id, src, hop) per rank.  A
+        rank that owns no block (more ranks than blocks) has nothing to run."""
+        out: list[list[np.ndarray]] = [[] for _ in range(self.world)]
+        self.rounds += 1
+        if self.lo == self.hi:
+            return [np.zeros((0, 4), np.uint32) for _ in range(self.world)]
         self.g.run(self.params)
         self.counts += self.g.read_counts().astype(np.uint64)
-        out: list[list[np.ndarray]] = [[] for _ in range(self.world)]
         for b in range(self.g.nblocks):
             if self.lo <= b < self.hi:
                 continue
@@ -95,7 +103,6 @@ class Partition:
             if len(recs):
                 out[int(self.owner[b])].append(recs)
         self.g.walks_clear()
-        self.rounds += 1
         res = [np.concatenate(o) if o else np.zeros((0, 4), np.uint32) for o in out]
         self.walks_sent += sum(len(r) for r in res)
         return res

@@ -103,6 +103,51 @@ def test_partitions_in_lock_step(oracle):
         assert not part.counts[outside].any()
 
 
+def test_more_ranks_than_blocks(oracle):
+    """Eight partitions of a five-block graph: three ranks own no block, run
+    nothing and receive nothing; the counts are still the oracle's."""
+    from oracle_blocks import OracleBlocks
+
+    from graphwalker_b200 import partitioned
+    from graphwalker_b200.engine import params
+    rp, ci = oracle.rmat_csr(10, 8, seed=3)
+    blocks = oracle.compute_blocks(rp, 7)
+    assert len(blocks) - 1 == 5
+    nv = len(rp) - 1
+    cur = np.arange(nv, dtype=np.uint32)
+    world = 8
+    parts = [partitioned.Partition(OracleBlocks(oracle, rp, ci, blocks), params(0, L=10, seed=1), r, world)
+             for r in range(world)]
+    assert sum(part.place(cur, ids=cur) for part in parts) == nv
+    while True:
+        outs = [part.step() for part in parts]
+        moved = 0
+        for r, part in enumerate(parts):
+            inc = np.concatenate([outs[s][r] for s in range(world)])
+            part.accept(inc)
+            moved += len(inc)
+        if moved == 0:
+            break
+    ref = oracle.run_walks(rp, ci, cur, ids=cur, src=cur, rule=0, L=10, seed=1)["counts"]
+    assert np.array_equal(sum(part.counts for part in parts), ref.astype(np.uint64))
+    assert sum(part.lo == part.hi for part in parts) == 3
+
+
+def test_partition_rejects_other_sinks_and_ranks(oracle):
+    import pytest
+
+    from oracle_blocks import OracleBlocks
+
+    from graphwalker_b200 import partitioned
+    from graphwalker_b200.engine import params
+    rp, ci = oracle.rmat_csr(10, 8, seed=3)
+    g = OracleBlocks(oracle, rp, ci, oracle.compute_blocks(rp, 12))
+    with pytest.raises(ValueError):
+        partitioned.Partition(g, params(0, sink=0, L=10), 0, 2)
+    with pytest.raises(ValueError):
+        partitioned.Partition(g, params(0, L=10), 2, 2)
+
+
 def test_owned_blocks_cover_every_block():
     from graphwalker_b200 import partitioned
     for nb in (1, 5, 33, 257):
