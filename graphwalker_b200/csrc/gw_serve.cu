@@ -417,9 +417,9 @@ gw_status gw_serve_open(gw_ctx* ctx, const gw_walk_params* params, const gw_serv
   }
   cudaError_t e = srv->tables.ensure(srv->cfg.table_slots * 8);
   if (e != cudaSuccess) {
+    const unsigned long long slots = srv->cfg.table_slots;
     delete srv;
-    return ctx->fail(GW_E_NOMEM, "serve table arena of %llu slots: %s",
-                     (unsigned long long)srv->cfg.table_slots, cudaGetErrorString(e));
+    return ctx->fail(GW_E_NOMEM, "serve table arena of %llu slots: %s", slots, cudaGetErrorString(e));
   }
   srv->arena.reset(srv->cfg.table_slots);
   srv->thread = std::thread(serve_loop, srv);
