@@ -106,3 +106,34 @@ def test_invalid_arguments_fail_cleanly():
     from graphwalker_b200._lib import GwError
     with pytest.raises(GwError):
         gw.Graph.open("/nonexistent/graph", 1024)
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """Every struct of include/graphwalker_b200.h has the same size and field
+    offsets in the Python binding (ctypes) as a C compiler gives it."""
+    import ctypes
+    import subprocess
+
+    from graphwalker_b200 import _lib
+    pairs = {"gw_walk_rec": _lib.WalkRec, "gw_walk_params": _lib.WalkParams, "gw_run_stats": _lib.RunStats,
+             "gw_graph_desc": _lib.GraphDesc, "gw_ppr_stats": _lib.PprStats, "gw_serve_config": _lib.ServeConfig,
+             "gw_serve_timing": _lib.ServeTiming, "gw_serve_stats": _lib.ServeStats,
+             "gw_convert_stats": _lib.ConvertStats}
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "graphwalker_b200.h"', "int main(void) {"]
+    for c, py in pairs.items():
+        lines.append(f'  printf("{c} size %zu\\n", sizeof({c}));')
+        for name, _ in py._fields_:
+            lines.append(f'  printf("{c} {name} %zu\\n", offsetof({c}, {name}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        c, field, v = line.split()
+        got[(c, field)] = int(v)
+    for c, py in pairs.items():
+        assert got[(c, "size")] == ctypes.sizeof(py), c
+        for name, _ in py._fields_:
+            assert got[(c, name)] == getattr(py, name).offset, (c, name)
