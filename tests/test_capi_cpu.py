@@ -137,3 +137,20 @@ def test_struct_layouts_match_the_header(tmp_path):
         assert got[(c, "size")] == ctypes.sizeof(py), c
         for name, _ in py._fields_:
             assert got[(c, name)] == getattr(py, name).offset, (c, name)
+
+
+def test_close_releases_every_context_buffer():
+    """gw_close frees every device and pinned buffer the context struct holds:
+    each gw_devbuf / gw_hostbuf member of gw_ctx is named in gw_close."""
+    ctx_h = (ROOT / "graphwalker_b200" / "csrc" / "gw_ctx.h").read_text()
+    body = re.search(r"struct gw_ctx \{(.*?)\n\};", ctx_h, re.S).group(1)
+    held = set()
+    for line in body.splitlines():
+        m = re.match(r"\s*gw_(?:dev|host)buf\s+([^;]*);", line.split("//")[0])
+        if m:
+            held |= {name.strip() for name in m.group(1).split(",")}
+    capi = (ROOT / "graphwalker_b200" / "csrc" / "gw_capi.cu").read_text()
+    start = capi.index("gw_status gw_close(gw_ctx* ctx)")
+    close = capi[start:capi.index("\n}\n", start)]
+    named = set(re.findall(r"ctx->(\w+)", close))
+    assert held and held <= named, sorted(held - named)
