@@ -144,11 +144,10 @@ def test_close_releases_every_context_buffer():
     each gw_devbuf / gw_hostbuf member of gw_ctx is named in gw_close."""
     ctx_h = (ROOT / "graphwalker_b200" / "csrc" / "gw_ctx.h").read_text()
     body = re.search(r"struct gw_ctx \{(.*?)\n\};", ctx_h, re.S).group(1)
+    code = "\n".join(line.split("//")[0] for line in body.splitlines())
     held = set()
-    for line in body.splitlines():
-        m = re.match(r"\s*gw_(?:dev|host)buf\s+([^;]*);", line.split("//")[0])
-        if m:
-            held |= {name.strip() for name in m.group(1).split(",")}
+    for decl in re.findall(r"\bgw_(?:dev|host)buf\s+([^;(){}]*);", code):
+        held |= {name.strip() for name in decl.split(",")}
     capi = (ROOT / "graphwalker_b200" / "csrc" / "gw_capi.cu").read_text()
     start = capi.index("gw_status gw_close(gw_ctx* ctx)")
     close = capi[start:capi.index("\n}\n", start)]
