@@ -68,6 +68,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-probe", action="store_true", help="skip the random-gather roof probe")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="rawwalk at N=1: skip the single-source PPR, msppr and serving sub-objects")
     ap.add_argument("--cpu-sample-sec", type=float, default=15.0)
     ap.add_argument("--workload", choices=["rawwalk", "msppr", "serve", "ppr1", "ooc", "convert", "simrank"],
                     default="rawwalk",
@@ -95,8 +97,16 @@ def workload_config(args, nblocks_actual=None) -> dict:
             "nvertices": 1 << args.scale, "walks_per_gpu": 1 << args.scale, "L": args.L,
             "nblocks": nblocks_actual if nblocks_actual is not None else args.nblocks,
             "blocksize_kb": blocksize_kb_for(args.scale, args.edge_factor, args.nblocks),
-            "rng": f"philox4x32-10 seed {args.walk_seed}", "l2": "flushed between steps (256 MB write)",
+            "l2": "flushed between steps (256 MB write)",
             "parallelism": f"replicated graph, walks sharded, dp{args.gpus}"}
+
+
+# Each arm names its random stream at the top level of its line, beside an
+# identical `config`: the engine draws from Philox keyed on (seed, walk id,
+# hop); the reference arm runs the reference unmodified, with glibc rand_r.
+RNG_OURS = "philox4x32-10 keyed (seed {seed}, walk id, hop): the deterministic mode, bit-exact to the shimmed reference"
+RNG_REFERENCE = ("glibc rand_r (native), seeded per block visit with walkid + dstId + hop + time(NULL) "
+                 "(randomwalkwithjump.hpp:37), as the reference runs")
 
 
 # --------------------------------------------------------------------------- clocks
@@ -195,21 +205,21 @@ def write_reference_graph(tmp: Path, args, rowptr, colidx) -> tuple[str, int, in
     return base, kb, len(blocks) - 1
 
 
-def make_graph_host(args):
-    """The benchmark graph on the host: generated on the GPU when one is
-    present (input preparation only), else by the C generator."""
-    import numpy as np
-    try:
-        import torch
-        if torch.cuda.is_available():
-            import graphwalker_b200 as gw
-            with gw.Graph.rmat(args.scale, args.edge_factor, seed=args.graph_seed,
-                               blocksize_kb=blocksize_kb_for(args.scale, args.edge_factor, args.nblocks)) as G:
-                return G.export_csr()
-    except ImportError:
-        pass
-    from oracle import py_oracle
-    return py_oracle.rmat_csr(args.scale, args.edge_factor, seed=args.graph_seed)
+def write_reference_graph_c(tmp: Path, args) -> tuple[str, int]:
+    """The benchmark graph for the reference arm, generated and written in the
+    reference's on-disk layout by the C generator (oracle/_build/gw_oracle_rmat,
+    the same seeded R-MAT stream the device generator reproduces bit for bit).
+    It runs as its own process, so the arm loads no library of this repository;
+    the reference computes the block range itself on its first run."""
+    exe = ROOT / "oracle" / "_build" / "gw_oracle_rmat"
+    if not exe.exists():
+        raise FileNotFoundError(f"{exe} missing (built by `make -C oracle`)")
+    base = str(tmp / f"rmat{args.scale}")
+    subprocess.run([str(exe), str(args.scale), str(args.edge_factor), str(args.graph_seed), "0.57", "0.19", "0.19",
+                    base], check=True, capture_output=True, timeout=1800)
+    (tmp / "conf").mkdir(exist_ok=True)
+    (tmp / "conf" / "graphwalker.cnf").write_text("# GraphWalker configuration (empty)\n")
+    return base, blocksize_kb_for(args.scale, args.edge_factor, args.nblocks)
 
 
 def host_cores() -> int:
@@ -219,7 +229,8 @@ def host_cores() -> int:
         return os.cpu_count() or 1
 
 
-def run_ref_bench(base, kb, nv, L, stride, warmup, steps, threads, cwd) -> list[tuple[int, float]]:
+def run_ref_bench(base, kb, nv, L, stride, warmup, steps, threads, cwd) -> list[tuple[int, float, int]]:
+    """(visits, seconds, OpenMP threads left at the end) per timed run."""
     exe = ROOT / "oracle" / "_ref" / "gw_ref_bench"
     if not exe.exists():
         raise FileNotFoundError(f"{exe} missing (built by `make -C oracle ref` where the reference tree exists)")
@@ -230,76 +241,135 @@ def run_ref_bench(base, kb, nv, L, stride, warmup, steps, threads, cwd) -> list[
     res = []
     for line in out.stdout.splitlines():
         f = line.split()
-        if len(f) == 8 and f[0] == "step":
-            res.append((int(f[3]) * L, float(f[7])))  # jump-rule walks make exactly L visits
+        if len(f) >= 10 and f[0] == "step":
+            res.append((int(f[3]) * L, float(f[7]), int(f[9])))  # jump-rule walks make exactly L visits
     return res
 
 
-def cpu_reference(args, rowptr, colidx, warmup: int, steps: int, budget_s: float) -> dict:
-    """Times the reference engine on the host cores; the per-run sample (one
-    walk on every `stride`-th vertex) is sized so warmup+steps runs fit budget_s."""
+def fallback_report(res, threads: int) -> dict:
+    """Whether the reference's sticky single-thread fallback fired: exec_updates
+    sets one OpenMP thread for a block with fewer than 100 walks and never
+    restores it (graphwalker.hpp:260)."""
+    fired = [i for i, r in enumerate(res) if threads > 1 and r[2] == 1]
+    return {"fired": bool(fired), "runs_fired": len(fired), "runs": len(res), "execthreads": threads,
+            "rule": "graphwalker.hpp:260 if(nwalks < 100) omp_set_num_threads(1), never undone within a run"}
+
+
+def cpu_reference(args, base: str, kb: int, nv: int, tmp: Path, warmup: int, steps: int, budget_s: float) -> dict:
+    """Times the reference engine on the host cores, on the graph files at
+    `base`; the per-run sample (one walk on every `stride`-th vertex) is sized
+    so that warmup + steps runs fit budget_s."""
     threads = host_cores()
-    with tempfile.TemporaryDirectory(prefix="gw_ref_") as td:
-        tmp = Path(td)
-        base, kb, nb = write_reference_graph(tmp, args, rowptr, colidx)
-        nv = len(rowptr) - 1
-        probe_stride = 64
-        cal = run_ref_bench(base, kb, nv, args.L, probe_stride, 1, 1, threads, tmp)
-        rate = cal[0][0] / max(cal[0][1], 1e-9)
-        per_step = budget_s / max(1, warmup + steps)
-        want_walks = max(1024, min(nv, int(rate * per_step / args.L)))
-        stride = max(1, nv // want_walks)
-        res = run_ref_bench(base, kb, nv, args.L, stride, warmup, steps, threads, tmp)
-    tot_steps = sum(s for s, _ in res)
-    tot_t = sum(t for _, t in res)
+    probe_stride = 64
+    cal = run_ref_bench(base, kb, nv, args.L, probe_stride, 1, 1, threads, tmp)
+    rate = cal[0][0] / max(cal[0][1], 1e-9)
+    per_step = budget_s / max(1, warmup + steps)
+    want_walks = max(1024, min(nv, int(rate * per_step / args.L)))
+    stride = max(1, nv // want_walks)
+    res = run_ref_bench(base, kb, nv, args.L, stride, warmup, steps, threads, tmp)
+    nb = len(Path(base + "_GraphWalker", f"blocksize_{kb}KB.blockrange").read_text().split()) - 1
+    tot_steps = sum(r[0] for r in res)
+    tot_t = sum(r[1] for r in res)
     return {"value": tot_steps / tot_t, "unit": METRIC, "cores": threads, "kind": "reference",
             "sec_per_step": tot_t / len(res), "steps": len(res), "nblocks": nb,
+            "single_thread_fallback": fallback_report(res, threads),
             "sample": f"the reference engine (graphwalker.hpp) + RandomWalkwithJump compiled -O3 from source, "
                       f"native rand_r, {threads} OpenMP threads, one walk on every {stride}-th vertex "
                       f"({nv // stride} walks x {args.L} hops per run) of the same scale-{args.scale} graph, "
                       f"blocks cached in RAM after the first run"}
 
 
-def cpu_reference_msppr(args, rowptr, colidx, walkspersource: int, budget_s: float) -> dict:
+def reference_parity(args, base: str, kb: int, blocks, nv: int, tmp: Path, gpu_counts) -> dict:
+    """The timed step's visit counts against the reference engine itself.
+
+    Runs GraphWalker's engine and RandomWalkwithJump, compiled from the
+    reference's sources with its rand_r calls routed to the same Philox stream
+    (oracle/_ref/gw_ref_shim_0), on the same graph files with the same walks:
+    one per vertex, source field = start vertex (its Philox key).  Outside the
+    timed region; `identical_counts` is the bit-for-bit comparison of all
+    per-vertex counts."""
+    import struct
+
+    import numpy as np
+    exe = ROOT / "oracle" / "_ref" / "gw_ref_shim_0"
+    if not exe.exists():
+        raise FileNotFoundError(f"{exe} missing (built by `make -C oracle ref` where the reference tree exists)")
+    if nv > (1 << 24):
+        raise ValueError("the walk word's 24-bit source field keys at most 2^24 walks")
+    threads = host_cores()
+    v = np.arange(nv, dtype=np.uint64)
+    b64 = np.asarray(blocks, dtype=np.int64)
+    blk = np.searchsorted(b64[1:], np.arange(nv, dtype=np.int64), side="right")
+    rec = np.zeros(nv, dtype=[("b", "<u4"), ("pad", "<u4"), ("w", "<u8")])
+    rec["b"] = blk
+    rec["w"] = (v << np.uint64(40)) | ((v - b64[blk].astype(np.uint64)) << np.uint64(14))  # walk.hpp:69-73, hop 0
+    wf, of = tmp / "parity_walks.bin", tmp / "parity_out.bin"
+    with open(wf, "wb") as f:
+        f.write(struct.pack("<Q", nv))
+        f.write(rec.tobytes())
+    del rec, v, blk
+    t0 = time.perf_counter()
+    subprocess.run([str(exe), base, str(kb), str(wf), str(of), str(args.L), f"{args.walk_seed:x}", str(nv), "0",
+                    "0.2", "0", "0", "execthreads", str(threads)], cwd=tmp, check=True, capture_output=True,
+                   timeout=1800)
+    sec = time.perf_counter() - t0
+    raw = of.read_bytes()
+    status, nv_ref = struct.unpack_from("<II", raw, 0)
+    ref = np.frombuffer(raw, np.uint32, nv_ref, 8)
+    gpu = np.asarray(gpu_counts, dtype=np.uint32)
+    diff = int(np.count_nonzero(ref != gpu)) if nv_ref == nv else nv
+    return {"identical_counts": bool(diff == 0 and status == 0), "vertices_differing": diff, "walks": nv,
+            "visits": int(ref.astype(np.int64).sum()), "reference_status": int(status), "sec": sec,
+            "against": "the reference engine + RandomWalkwithJump compiled from source, rand_r routed to the same "
+                       "Philox stream (gw_ref_shim_0), all walks of the timed step, counts of its last step"}
+
+
+def cpu_reference_msppr(args, base: str, kb: int, nv: int, tmp: Path, walkspersource: int, budget_s: float) -> dict:
     """The reference engine with RandomWalkwithStop on msppr's placement
     (contiguous sources, a fixed number of walks each), sized to budget_s."""
     threads = host_cores()
     exe = ROOT / "oracle" / "_ref" / "gw_ref_bench"
-    with tempfile.TemporaryDirectory(prefix="gw_ref_") as td:
-        tmp = Path(td)
-        base, kb, nb = write_reference_graph(tmp, args, rowptr, colidx)
-        nv = len(rowptr) - 1
+    if not exe.exists():
+        raise FileNotFoundError(f"{exe} missing (built by `make -C oracle ref` where the reference tree exists)")
 
-        def run(numsources: int, warm: int):
-            out = subprocess.run([str(exe), base, str(kb), str(nv), "20", "1", str(warm), "1", "execthreads",
-                                  str(threads), "msppr", "0", str(numsources), str(walkspersource)],
-                                 cwd=tmp, capture_output=True, text=True, timeout=1800)
-            if out.returncode != 0:
-                raise RuntimeError(out.stderr[-400:])
-            f = [l.split() for l in out.stdout.splitlines() if l.startswith("step")][-1]
-            return float(f[7]), int(f[5])
+    def run(numsources: int, warm: int):
+        out = subprocess.run([str(exe), base, str(kb), str(nv), "20", "1", str(warm), "1", "execthreads",
+                              str(threads), "msppr", "0", str(numsources), str(walkspersource)],
+                             cwd=tmp, capture_output=True, text=True, timeout=1800)
+        if out.returncode != 0:
+            raise RuntimeError(out.stderr[-400:])
+        f = [l.split() for l in out.stdout.splitlines() if l.startswith("step")][-1]
+        return float(f[7]), int(f[5]), int(f[9])
 
-        t_cal, _ = run(8, 1)
-        numsources = max(8, min(4096, int(8 * budget_s / max(t_cal, 1e-6))))
-        t, visits = run(numsources, 1)
+    t_cal, _, _ = run(8, 1)
+    numsources = max(8, min(4096, int(8 * budget_s / max(t_cal, 1e-6))))
+    t, visits, thr_after = run(numsources, 1)
     return {"value": numsources / t, "unit": "queries/s", "cores": threads, "kind": "reference",
+            "single_thread_fallback": fallback_report([(visits, t, thr_after)], threads),
             "sample": f"the reference engine + RandomWalkwithStop compiled -O3 from source, native rand_r, "
                       f"{threads} OpenMP threads, msppr placement: sources 0..{numsources - 1} x {walkspersource} "
                       f"walks (the mean budget), L<=20, a per-thread visit counter as sink ({visits} visits)"}
 
 
 def reference_arm(args) -> None:
+    """The reference's CPU engine on this box's host cores, on the headline
+    workload.  Nothing of this repository's engine is loaded: the graph comes
+    from the C generator (its own process) and the timed binary is the
+    reference compiled from its sources."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    rowptr, colidx = make_graph_host(args)
     warm = max(1, args.warmup)
-    r = cpu_reference(args, rowptr, colidx, warm, args.steps, budget_s=150.0)
+    with tempfile.TemporaryDirectory(prefix="gw_ref_") as td:
+        tmp = Path(td)
+        base, kb = write_reference_graph_c(tmp, args)
+        r = cpu_reference(args, base, kb, 1 << args.scale, tmp, warm, args.steps, budget_s=150.0)
     line = {"metric": METRIC, "value": r["value"], "unit": METRIC, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": warm, "ms_per_step": r["sec_per_step"] * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": workload_config(args, r["nblocks"]),
+            "config": workload_config(args, r["nblocks"]), "rng": RNG_REFERENCE,
             "cpu_baseline": {"value": r["value"], "unit": METRIC, "cores": r["cores"], "kind": "reference",
                              "sample": r["sample"]},
+            "single_thread_fallback": r["single_thread_fallback"],
             "e2e": {"value": r["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -330,6 +400,7 @@ def our_arm(args) -> None:
     # walk records resident in HBM: one walk per vertex, ids offset by rank
     v = torch.arange(nv, dtype=torch.int64, device="cuda")
     walks = torch.stack([v, v + rank * nv, v, torch.zeros_like(v)], dim=1).to(torch.int32).contiguous()
+    del v
     counts = torch.zeros(nv, dtype=torch.int32, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     p = gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, L, seed=args.walk_seed, aggregate=bool(args.aggregate))
@@ -337,16 +408,15 @@ def our_arm(args) -> None:
     # launch shape (CTAs per SM) timed on these walks before the warm-up
     tuned_ctas = G.walk_autotune(p, walks, nv)
 
-    def step():
-        counts.zero_()
-        G.walk_device(p, walks, nv, counts=counts, stream=sh)
-
     def barrier():
         if world > 1:
             dist.barrier(device_ids=[local])
 
+    # A step = clear the counts, walk every walk to its end, and (N > 1) sum
+    # the counts over the ranks: the path's one exchange is inside the step.
     for _ in range(max(3, args.warmup)):
-        step()
+        counts.zero_()
+        G.walk_device(p, walks, nv, counts=counts, stream=sh)
         if world > 1:
             dist.all_reduce(counts)
     G.sync(sh)
@@ -356,7 +426,7 @@ def our_arm(args) -> None:
         raise RuntimeError(f"visit count {total_visits} != {expect}")
 
     K = args.steps
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(K)]
     with ClockSampler(device_uuid(local)) as clk:
         barrier()
         torch.cuda.synchronize()
@@ -368,18 +438,21 @@ def our_arm(args) -> None:
             G.walk_device(p, walks, nv, counts=counts, stream=sh)
             ev[k][2].record(stream)
             if world > 1:
-                dist.all_reduce(counts)
+                dist.all_reduce(counts)  # blocking form: the current stream waits for the reduction
+            ev[k][3].record(stream)
         torch.cuda.synchronize()
         barrier()
     G.sync(sh)
-    step_ms = sum(e[0].elapsed_time(e[2]) for e in ev) / K
+    step_ms = sum(e[0].elapsed_time(e[3]) for e in ev) / K
     kern_ms = sum(e[1].elapsed_time(e[2]) for e in ev) / K
+    xchg_ms = sum(e[2].elapsed_time(e[3]) for e in ev) / K
     if world > 1:
-        t = torch.tensor([step_ms, kern_ms], dtype=torch.float64, device="cuda")
+        t = torch.tensor([step_ms, kern_ms, xchg_ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms, kern_ms = t.tolist()
+        step_ms, kern_ms, xchg_ms = t.tolist()
     steps_per_launch = nv * L
     value = steps_per_launch * world / (step_ms * 1e-3)
+    last_counts = counts.cpu().numpy().view(np.uint32).copy() if world == 1 else None
 
     # random-sector gather roof: an 8 GB buffer, far larger than L2
     gather_bps = None
@@ -392,42 +465,22 @@ def our_arm(args) -> None:
     # e2e through the C-ABI host call (pinned words in, counts out)
     e2e = None
     if not args.no_e2e:
-        vv = np.arange(nv, dtype=np.uint64)
-        blocks = G.blocks.astype(np.int64)
-        blk = np.searchsorted(blocks[1:], np.arange(nv), side="right")
-        words_np = gw.encode(vv, vv - blocks[blk].astype(np.uint64), 0)
-        offs_np = np.r_[0, np.cumsum(np.bincount(blk, minlength=G.nblocks))].astype(np.uint64)
-        words = torch.from_numpy(words_np.view(np.int64)).pin_memory()
-        offs = torch.from_numpy(offs_np.view(np.int64)).pin_memory()
-        ids = None
-        if rank:
-            ids = torch.from_numpy((np.arange(nv, dtype=np.uint64) + rank * nv).astype(np.uint32).view(np.int32)).pin_memory()
-        hcounts = torch.zeros(nv, dtype=torch.int32).pin_memory()
-        for _ in range(3):
-            G.run_pools(p, words.data_ptr(), offs.data_ptr(), hcounts.data_ptr(), ids=None if ids is None else ids.data_ptr())
-        barrier()
-        t0 = time.perf_counter()
-        n_e2e = min(K, 50)
-        for _ in range(n_e2e):
-            G.run_pools(p, words.data_ptr(), offs.data_ptr(), hcounts.data_ptr(), ids=None if ids is None else ids.data_ptr())
-        e2e_s = (time.perf_counter() - t0) / n_e2e
-        if world > 1:
-            t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = t.item()
-        if int(hcounts.numpy().view(np.uint32).astype(np.int64).sum()) != nv * L:
-            raise RuntimeError("e2e visit count mismatch")
-        e2e = {"value": steps_per_launch * world / e2e_s, "unit": METRIC,
-               "h2d_bytes_per_step": int(words.numel() * 8 + offs.numel() * 8 + (ids.numel() * 4 if ids is not None else 0)),
-               "d2h_bytes_per_step": int(nv * 4), "ms_per_step": e2e_s * 1e3,
-               "api": "gw_run_pools (C ABI, pinned host buffers)"}
+        e2e = e2e_run_pools(args, G, p, rank, world, K, barrier, last_counts)
 
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             rowptr, colidx = G.export_csr()
-            cpu = cpu_reference(args, rowptr, colidx, 1, 1, budget_s=args.cpu_sample_sec)
-            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            with tempfile.TemporaryDirectory(prefix="gw_ref_") as td:
+                tmp = Path(td)
+                base, kbw, _ = write_reference_graph(tmp, args, rowptr, colidx)
+                del rowptr, colidx
+                r = cpu_reference(args, base, kbw, nv, tmp, 1, 1, budget_s=args.cpu_sample_sec)
+                cpu = {k: r[k] for k in ("value", "unit", "cores", "kind", "sample", "single_thread_fallback")}
+                try:
+                    parity = reference_parity(args, base, kbw, G.blocks, nv, tmp, last_counts)
+                except Exception as exc:  # reported, never required
+                    parity = {"identical_counts": None, "error": str(exc)[-300:]}
         except Exception as exc:  # the baseline is reported, never required
             cpu = {"value": None, "unit": METRIC, "cores": host_cores(), "kind": "reference",
                    "sample": f"unavailable: {exc}"}
@@ -435,8 +488,10 @@ def our_arm(args) -> None:
     if world > 1:
         dist.barrier(device_ids=[local])
         dist.destroy_process_group()
+    G.close()
+    del walks, counts, flush
+    torch.cuda.empty_cache()
     if rank != 0:
-        G.close()
         return
     peak, peak_kind = measured_peaks()
     algo_bytes = BYTES_PER_STEP[layout] * steps_per_launch + BYTES_PER_WALK[layout] * nv
@@ -454,12 +509,71 @@ def our_arm(args) -> None:
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
             "warmup": max(3, args.warmup), "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {**workload_config(args, G.nblocks), "graph_layout": layout,
-                       "autotuned_ctas_per_sm": tuned_ctas},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": K, "clocks": clk.summary(),
-            "walk_steps_per_step": steps_per_launch * world}
-    G.close()
+            "config": workload_config(args, G.nblocks), "rng": RNG_OURS.format(seed=args.walk_seed),
+            "engine": {"graph_layout": layout, "autotuned_ctas_per_sm": tuned_ctas},
+            "step_breakdown_ms": {"walk_kernel": kern_ms, "count_exchange": xchg_ms,
+                                  "exchange": "NCCL all_reduce of the u32 counts" if world > 1 else "none (N=1)"},
+            "roofline": roof, "cpu_baseline": cpu, "parity": parity, "e2e": e2e, "gpu_launches": K,
+            "clocks": clk.summary(), "walk_steps_per_step": steps_per_launch * world}
+    if world == 1 and not args.no_extras:
+        # the other configs' workloads, each measured in this same run
+        for key, fn in (("ppr1", ppr1_measure), ("msppr", msppr_measure),
+                        ("serve", lambda a: serve_measure(a, rates="1000,10000,50000"))):
+            t0 = time.perf_counter()
+            try:
+                line[key] = fn(args)
+            except Exception as exc:  # reported, never required
+                line[key] = {"error": f"{type(exc).__name__}: {str(exc)[-300:]}"}
+            line[key]["wall_s"] = time.perf_counter() - t0
+            torch.cuda.empty_cache()
     print(json.dumps(line), flush=True)
+
+
+def e2e_run_pools(args, G, p, rank: int, world: int, K: int, barrier, device_counts) -> dict:
+    """The headline metric through the C-ABI host call a program makes
+    (gw_run_pools): 64-bit walk words copied in from pinned host memory and the
+    u32 counts copied back, every step."""
+    import numpy as np
+    import torch
+
+    import graphwalker_b200 as gw
+    nv, L = G.nv, args.L
+    vv = np.arange(nv, dtype=np.uint64)
+    blocks = G.blocks.astype(np.int64)
+    blk = np.searchsorted(blocks[1:], np.arange(nv), side="right")
+    words_np = gw.encode(vv, vv - blocks[blk].astype(np.uint64), 0)
+    offs_np = np.r_[0, np.cumsum(np.bincount(blk, minlength=G.nblocks))].astype(np.uint64)
+    words = torch.from_numpy(words_np.view(np.int64)).pin_memory()
+    offs = torch.from_numpy(offs_np.view(np.int64)).pin_memory()
+    del vv, blk, words_np
+    ids = None
+    if rank:
+        ids = torch.from_numpy((np.arange(nv, dtype=np.uint64) + rank * nv).astype(np.uint32).view(np.int32)).pin_memory()
+    hcounts = torch.zeros(nv, dtype=torch.int32).pin_memory()
+    idp = None if ids is None else ids.data_ptr()
+    for _ in range(3):
+        G.run_pools(p, words.data_ptr(), offs.data_ptr(), hcounts.data_ptr(), ids=idp)
+    barrier()
+    n_e2e = min(K, 50)
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        G.run_pools(p, words.data_ptr(), offs.data_ptr(), hcounts.data_ptr(), ids=idp)
+    e2e_s = (time.perf_counter() - t0) / n_e2e
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = t.item()
+    got = hcounts.numpy().view(np.uint32)
+    if int(got.astype(np.int64).sum()) != nv * L:
+        raise RuntimeError("e2e visit count mismatch")
+    out = {"value": nv * L * world / e2e_s, "unit": METRIC,
+           "h2d_bytes_per_step": int(words.numel() * 8 + offs.numel() * 8 + (ids.numel() * 4 if ids is not None else 0)),
+           "d2h_bytes_per_step": int(nv * 4), "ms_per_step": e2e_s * 1e3,
+           "api": "gw_run_pools (C ABI, pinned host buffers)"}
+    if device_counts is not None:
+        out["identical_to_device_step"] = bool(np.array_equal(got, device_counts))
+    return out
 
 
 def msppr_queries(rp, nq: int, seed: int = 7):
@@ -473,79 +587,120 @@ def msppr_queries(rp, nq: int, seed: int = 7):
     return sources, budgets
 
 
-def msppr_arm(args) -> None:
+def extra_scale(args, default: int) -> int:
+    """The graph scale of a non-headline workload: its config's own, unless
+    --scale names another than the headline's 24."""
+    return args.scale if args.scale != 24 else default
+
+
+def msppr_measure(args) -> dict:
     """Batched multi-source PPR (one persistent launch for all queries) vs the
-    plain per-query path, on one GPU: queries/s, same results."""
+    plain per-query path, on one GPU: queries/s, same results, and the top-100
+    accuracy of the largest queries judged against the FP64 power series."""
     import numpy as np
     import torch
 
     import graphwalker_b200 as gw
+    from graphwalker_b200 import accuracy
     torch.cuda.set_device(0)
-    scale = args.scale if args.scale != 24 else 26
+    scale = extra_scale(args, 26)
     kb = blocksize_kb_for(scale, args.edge_factor, args.nblocks)
     G = gw.Graph.rmat(scale, args.edge_factor, seed=args.graph_seed, blocksize_kb=kb)
-    layout = "erec" if G.set_edge_records(LAYOUT_MODE[args.layout]) else "csr"
-    rp, _ = G.export_csr()
-    sources, budgets = msppr_queries(rp, args.queries)
-    del rp
-    p = gw.params(gw.RULE_STOP, gw.SINK_NONE, 20, seed=args.walk_seed)
-    tuned, tuned_chunk = G.ppr_autotune(p, sources[:256], budgets[:256])
-    for _ in range(max(1, args.warmup)):
-        G.ppr(p, sources, budgets, k=args.topk, batched=True)
-    runs = []
-    with ClockSampler(device_uuid(0)) as clk:
-        for _ in range(args.steps):
-            ids_b, cnt_b, st = G.ppr(p, sources, budgets, k=args.topk, batched=True)
-            runs.append((st.ms_total, st.ms_clear, st.ms_walk, st.ms_topk))
-    ms = [r[0] for r in runs]
-    ms_med = statistics.median(ms)
-    G.ppr(p, sources, budgets, k=args.topk, batched=False)  # warm-up of the plain path
-    ids_p, cnt_p, stp = G.ppr(p, sources, budgets, k=args.topk, batched=False)
-    same = bool(np.array_equal(ids_b, ids_p) and np.array_equal(cnt_b, cnt_p))
-    t0 = time.perf_counter()
-    G.ppr(p, sources, budgets, k=args.topk, batched=True)
-    e2e_s = time.perf_counter() - t0
-    # top-100 accuracy against the FP64 power series, on the largest-budget queries
-    acc = []
-    for q in np.argsort(-budgets.astype(np.int64))[:4]:
-        mu = G.expected_visits(p, int(sources[q]))
-        exact = set(np.argsort(-mu, kind="stable")[:args.topk].tolist())
-        got = set(int(x) for x in ids_b[q] if x != 0xFFFFFFFF)
-        acc.append({"budget": int(budgets[q]), "top_overlap": len(exact & got)})
-    cpu = None
-    if not args.no_cpu_baseline:
-        try:
-            rp_h, ci_h = G.export_csr()
-            cpu = cpu_reference_msppr(args, rp_h, ci_h, int(round(float(budgets.mean()))), args.cpu_sample_sec)
-            del rp_h, ci_h
-        except Exception as exc:  # reported, never required
-            cpu = {"value": None, "unit": "queries/s", "cores": host_cores(), "kind": "reference",
-                   "sample": f"unavailable: {exc}"}
-    line = {"metric": "queries/s", "value": args.queries / (ms_med * 1e-3), "unit": "queries/s",
-            "workload": "msppr", "n_gpus": 1, "steps": args.steps, "warmup": max(1, args.warmup),
-            "ms_per_step": ms_med, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u32", "data": "synthetic",
-            "config": {"workload": f"multi-source PPR, R-MAT scale {scale} ef {args.edge_factor}, {args.queries} queries, "
-                                   f"sources uniform over out-degree>=1, budgets round(10^U(2,5)), stop rule p=0.15, "
-                                   f"L<=20, top-{args.topk}",
-                       "walks_per_step": int(budgets.sum()), "autotuned_threads_per_sm": tuned,
-                       "autotuned_walks_per_warp_grab": tuned_chunk,
-                       "graph_layout": layout},
-            "breakdown_ms": {"clear": statistics.median(r[1] for r in runs),
-                             "walk": statistics.median(r[2] for r in runs),
-                             "topk": statistics.median(r[3] for r in runs)},
-            "plain": {"value": args.queries / (stp.ms_total * 1e-3), "unit": "queries/s", "ms": stp.ms_total,
-                      "launches": stp.launches},
-            "speedup_vs_plain": stp.ms_total / ms_med, "identical_to_plain": same,
-            "accuracy_vs_fp64": acc, "cpu_baseline": cpu,
-            "e2e": {"value": args.queries / e2e_s, "unit": "queries/s", "api": "gw_ppr_run (host arrays)",
-                    "h2d_bytes_per_step": int(args.queries * 8), "d2h_bytes_per_step": int(args.queries * args.topk * 8)},
-            "gpu_launches": int(st.launches) * args.steps, "clocks": clk.summary()}
-    G.close()
+    try:
+        layout = "erec" if G.set_edge_records(LAYOUT_MODE[args.layout]) else "csr"
+        rp, _ = G.export_csr()
+        sources, budgets = msppr_queries(rp, args.queries)
+        del rp
+        L = 20
+        p = gw.params(gw.RULE_STOP, gw.SINK_NONE, L, seed=args.walk_seed)
+        tuned, tuned_chunk = G.ppr_autotune(p, sources[:256], budgets[:256])
+        for _ in range(max(1, args.warmup)):
+            G.ppr(p, sources, budgets, k=args.topk, batched=True)
+        runs = []
+        steps = max(1, args.steps)
+        with ClockSampler(device_uuid(0)) as clk:
+            for _ in range(steps):
+                ids_b, cnt_b, st = G.ppr(p, sources, budgets, k=args.topk, batched=True)
+                runs.append((st.ms_total, st.ms_clear, st.ms_walk, st.ms_topk))
+        ms_med = statistics.median(r[0] for r in runs)
+        G.ppr(p, sources, budgets, k=args.topk, batched=False)  # warm-up of the plain path
+        ids_p, cnt_p, stp = G.ppr(p, sources, budgets, k=args.topk, batched=False)
+        same = bool(np.array_equal(ids_b, ids_p) and np.array_equal(cnt_b, cnt_p))
+        e2e = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            G.ppr(p, sources, budgets, k=args.topk, batched=True)
+            e2e.append(time.perf_counter() - t0)
+        e2e_s = statistics.median(e2e)
+        # top-100 accuracy of the largest-budget queries against the FP64 power
+        # series, judged against the Monte Carlo noise of their budgets.  The
+        # full per-vertex counts come from the same walks (walk j of the batch
+        # has Philox id j) run through the resident kernel.
+        prefix = np.r_[0, np.cumsum(budgets.astype(np.int64))]
+        acc = []
+        for q in np.argsort(-budgets.astype(np.int64), kind="stable")[:4]:
+            src, B = int(sources[q]), int(budgets[q])
+            mu = G.expected_visits(p, src)
+            j = torch.arange(prefix[q], prefix[q + 1], dtype=torch.int64, device="cuda")
+            w = torch.stack([torch.full_like(j, src), j, torch.full_like(j, src), torch.zeros_like(j)], 1)
+            w = w.to(torch.int32).contiguous()
+            cnt = torch.zeros(G.nv, dtype=torch.int32, device="cuda")
+            G.walk_device(gw.params(gw.RULE_STOP, gw.SINK_VERTEX_COUNT, L, seed=args.walk_seed), w, B, counts=cnt)
+            G.sync()
+            c = cnt.cpu().numpy().view(np.uint32)
+            del w, cnt, j
+            nz = np.flatnonzero(c)
+            from_counts = accuracy.count_topk(nz, c[nz], args.topk)
+            listed = ids_b[q][ids_b[q] != 0xFFFFFFFF]
+            m = accuracy.measured_accuracy(mu, B, L, ids_b[q], counts=c, k=args.topk)
+            m["query"] = int(q)
+            m["batched_list_equals_counts_topk"] = bool(np.array_equal(listed, from_counts))
+            acc.append(m)
+        cpu = None
+        if not args.no_cpu_baseline:
+            try:
+                rp_h, ci_h = G.export_csr()
+                with tempfile.TemporaryDirectory(prefix="gw_ref_") as td:
+                    tmp = Path(td)
+                    base, kbw, _ = write_reference_graph(tmp, argparse.Namespace(**{**vars(args), "scale": scale}),
+                                                         rp_h, ci_h)
+                    del rp_h, ci_h
+                    cpu = cpu_reference_msppr(args, base, kbw, G.nv, tmp, int(round(float(budgets.mean()))),
+                                              args.cpu_sample_sec)
+            except Exception as exc:  # reported, never required
+                cpu = {"value": None, "unit": "queries/s", "cores": host_cores(), "kind": "reference",
+                       "sample": f"unavailable: {exc}"}
+        return {"metric": "queries/s", "value": args.queries / (ms_med * 1e-3), "unit": "queries/s",
+                "workload": "msppr", "n_gpus": 1, "steps": steps, "warmup": max(1, args.warmup),
+                "ms_per_step": ms_med, "higher_is_better": True, "dtype": "u32", "data": "synthetic",
+                "config": {"workload": f"multi-source PPR, R-MAT scale {scale} ef {args.edge_factor}, "
+                                       f"{args.queries} queries, sources uniform over out-degree>=1, budgets "
+                                       f"round(10^U(2,5)), stop rule p=0.15, L<=20, top-{args.topk}",
+                           "walks_per_step": int(budgets.sum()), "autotuned_threads_per_sm": tuned,
+                           "autotuned_walks_per_warp_grab": tuned_chunk, "graph_layout": layout},
+                "breakdown_ms": {"clear": statistics.median(r[1] for r in runs),
+                                 "walk": statistics.median(r[2] for r in runs),
+                                 "topk": statistics.median(r[3] for r in runs)},
+                "plain": {"value": args.queries / (stp.ms_total * 1e-3), "unit": "queries/s", "ms": stp.ms_total,
+                          "launches": stp.launches},
+                "speedup_vs_plain": stp.ms_total / ms_med, "identical_to_plain": same,
+                "accuracy_vs_fp64": acc, "cpu_baseline": cpu,
+                "e2e": {"value": args.queries / e2e_s, "unit": "queries/s", "ms_per_step": e2e_s * 1e3,
+                        "api": "gw_ppr_run (host arrays in, top-k lists out)",
+                        "h2d_bytes_per_step": int(args.queries * 8),
+                        "d2h_bytes_per_step": int(args.queries * args.topk * 8)},
+                "gpu_launches": int(st.launches) * steps, "clocks": clk.summary()}
+    finally:
+        G.close()
+
+
+def msppr_arm(args) -> None:
+    line = msppr_measure(args)
+    line["scaling"], line["vs_baseline"] = "weak", None
     print(json.dumps(line), flush=True)
 
 
-def serve_arm(args) -> None:
+def serve_measure(args, rates: str | None = None) -> dict:
     """PPR serving on one GPU: Poisson arrivals at each rate, budgets
     Pareto(alpha=1.5, x_m=100) clipped to [100, 1e6], top-100 per query;
     continuous batching vs the plain one-query-per-superstep server."""
@@ -554,117 +709,135 @@ def serve_arm(args) -> None:
 
     import graphwalker_b200 as gw
     torch.cuda.set_device(0)
-    scale = args.scale if args.scale != 24 else 26
+    scale = extra_scale(args, 26)
     G = gw.Graph.rmat(scale, args.edge_factor, seed=args.graph_seed,
                       blocksize_kb=blocksize_kb_for(scale, args.edge_factor, args.nblocks))
-    rp, _ = G.export_csr()
-    deg = np.diff(rp.astype(np.int64))
-    cand = np.nonzero(deg > 0)[0]
-    del rp, deg
-    p = gw.params(gw.RULE_STOP, gw.SINK_NONE, 20, seed=args.walk_seed)
-    rng = np.random.default_rng(11)
-    G.ppr_autotune(p, rng.choice(cand, 64).astype(np.uint32), np.full(64, 2000, np.uint32))
-    results = []
-    for rate in [float(r) for r in args.rates.split(",")]:
-        n = max(200, int(rate * args.serve_sec))
-        src = rng.choice(cand, n).astype(np.uint32)
-        bud = np.clip(np.round(100.0 / rng.random(n) ** (1 / 1.5)), 100, 1_000_000).astype(np.uint32)
-        gaps = rng.exponential(1e9 / rate, n)
-        row = {"rate_qps": rate, "queries": n, "mean_budget": float(bud.mean())}
-        for name, mode in (("batched", gw._lib.SERVE_BATCHED), ("plain", gw._lib.SERVE_PLAIN)):
-            with G.serve(p, k=args.topk, mode=mode, table_slots=1 << 30) as S:
-                S.wait(S.submit(int(src[0]), 1000, 0))  # warm-up
-                t0 = S.clock_ns() + 5_000_000
-                arrivals = t0 + np.cumsum(gaps).astype(np.int64)
-                tickets = [S.submit(int(s), int(b), i, int(a)) for i, (s, b, a) in enumerate(zip(src, bud, arrivals))]
-                tm = [S.wait(t)[2] for t in tickets]
-                st = S.stats()
-            lat = np.array([x.done_ns - x.arrival_ns for x in tm], dtype=np.float64) / 1e6
-            span = (max(x.done_ns for x in tm) - int(arrivals[0])) / 1e9
-            row[name] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                         "throughput_qps": n / span, "supersteps": int(st.supersteps)}
-        results.append(row)
-        print(json.dumps(row), flush=True)
-    best = max(results, key=lambda r: r["batched"]["throughput_qps"])
-    line = {"metric": "queries/s", "value": best["batched"]["throughput_qps"], "unit": "queries/s",
-            "workload": "serve", "n_gpus": 1, "steps": len(results), "warmup": 1, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": f"PPR serving, R-MAT scale {scale}, Poisson arrivals, budgets Pareto(1.5, 100) "
-                                   f"clipped to [100, 1e6], stop rule p=0.15, L<=20, top-{args.topk}"},
-            "rates": results}
-    G.close()
+    try:
+        rp, _ = G.export_csr()
+        deg = np.diff(rp.astype(np.int64))
+        cand = np.nonzero(deg > 0)[0]
+        del rp, deg
+        p = gw.params(gw.RULE_STOP, gw.SINK_NONE, 20, seed=args.walk_seed)
+        rng = np.random.default_rng(11)
+        G.ppr_autotune(p, rng.choice(cand, 64).astype(np.uint32), np.full(64, 2000, np.uint32))
+        results = []
+        with ClockSampler(device_uuid(0)) as clk:
+            for rate in [float(r) for r in (rates or args.rates).split(",")]:
+                n = max(200, int(rate * args.serve_sec))
+                src = rng.choice(cand, n).astype(np.uint32)
+                bud = np.clip(np.round(100.0 / rng.random(n) ** (1 / 1.5)), 100, 1_000_000).astype(np.uint32)
+                gaps = rng.exponential(1e9 / rate, n)
+                row = {"rate_qps": rate, "queries": n, "mean_budget": float(bud.mean())}
+                lists = {}
+                for name, mode in (("batched", gw._lib.SERVE_BATCHED), ("plain", gw._lib.SERVE_PLAIN)):
+                    with G.serve(p, k=args.topk, mode=mode, table_slots=1 << 30) as S:
+                        S.wait(S.submit(int(src[0]), 1000, 0), 60_000)  # warm-up
+                        t0 = S.clock_ns() + 5_000_000
+                        arrivals = t0 + np.cumsum(gaps).astype(np.int64)
+                        tickets = [S.submit(int(s), int(b), i, int(a))
+                                   for i, (s, b, a) in enumerate(zip(src, bud, arrivals))]
+                        res = [S.wait(t, 600_000) for t in tickets]
+                        st = S.stats()
+                    tm = [r[2] for r in res]
+                    lists[name] = np.stack([r[0] for r in res])
+                    lat = np.array([x.done_ns - x.arrival_ns for x in tm], dtype=np.float64) / 1e6
+                    span = (max(x.done_ns for x in tm) - int(arrivals[0])) / 1e9
+                    row[name] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                                 "throughput_qps": n / span, "supersteps": int(st.supersteps)}
+                # a query's draws depend only on (source, budget, stream): same lists either way
+                row["identical_lists_batched_vs_plain"] = bool(np.array_equal(lists["batched"], lists["plain"]))
+                results.append(row)
+        best = max(results, key=lambda r: r["batched"]["throughput_qps"])
+        return {"metric": "queries/s", "value": best["batched"]["throughput_qps"], "unit": "queries/s",
+                "workload": "serve", "n_gpus": 1, "steps": len(results), "warmup": 1, "higher_is_better": True,
+                "dtype": "u32", "data": "synthetic",
+                "config": {"workload": f"PPR serving, R-MAT scale {scale}, Poisson arrivals, budgets Pareto(1.5, 100) "
+                                       f"clipped to [100, 1e6], stop rule p=0.15, L<=20, top-{args.topk}, "
+                                       f"{args.serve_sec} s of arrivals per rate"},
+                "rates": results, "clocks": clk.summary()}
+    finally:
+        G.close()
+
+
+def serve_arm(args) -> None:
+    line = serve_measure(args)
+    line["scaling"], line["vs_baseline"] = "weak", None
     print(json.dumps(line), flush=True)
 
 
-def ppr1_arm(args) -> None:
+def ppr1_measure(args) -> dict:
     """Single-source PPR (R-MAT scale 20, 16 blocks, 100,000 walks from vertex
     0, stop w.p. 0.15, a dangling vertex sends the walk back to its source,
     at most 20 hops): per-vertex visit counts and the top-100, with the L1
-    error and top-100 overlap against the FP64 power series."""
+    error and top-100 overlap judged against the FP64 power series."""
     import numpy as np
     import torch
 
     import graphwalker_b200 as gw
+    from graphwalker_b200 import accuracy
     torch.cuda.set_device(0)
-    scale = 20 if args.scale == 24 else args.scale
+    scale = extra_scale(args, 20)
     B, L = 100_000, 20
     G = gw.Graph.rmat(scale, args.edge_factor, seed=args.graph_seed,
                       blocksize_kb=blocksize_kb_for(scale, args.edge_factor, 16))
-    nv = G.nv
-    # "vertex 0" of the R-MAT generator (all-zero quadrant bits: its hub) is
-    # the vertex with the largest out-degree once ids are permuted
-    rp, _ = G.export_csr()
-    src = int(np.argmax(np.diff(rp.astype(np.int64))))
-    del rp
-    j = torch.arange(B, dtype=torch.int64, device="cuda")
-    walks = torch.stack([torch.full_like(j, src), j, torch.full_like(j, src), torch.zeros_like(j)], 1)
-    walks = walks.to(torch.int32).contiguous()
-    counts = torch.zeros(nv, dtype=torch.int32, device="cuda")
-    p = gw.params(gw.RULE_PPR, gw.SINK_VERTEX_COUNT, L, seed=args.walk_seed, aggregate=True)
-    sh = torch.cuda.current_stream().cuda_stream
-    for _ in range(max(3, args.warmup)):
-        counts.zero_()
-        G.walk_device(p, walks, B, counts=counts, stream=sh)
-    G.sync(sh)
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for a, b in ev:
-        counts.zero_()
-        a.record()
-        G.walk_device(p, walks, B, counts=counts, stream=sh)
-        b.record()
-    G.sync(sh)
-    ms = statistics.median(a.elapsed_time(b) for a, b in ev)
-    c = counts.cpu().numpy().view(np.uint32).astype(np.float64)
-    steps = int(c.sum())
-    # the same query through the C ABI (gw_ppr_run, host arrays in and out): warm calls
-    api_dev, api_wall = [], []
-    for i in range(3 + max(1, args.steps)):
-        t0 = time.perf_counter()
-        ids, cnt, st = G.ppr(p, np.array([src], np.uint32), np.array([B], np.uint32), k=100)
-        if i >= 3:
-            api_wall.append((time.perf_counter() - t0) * 1e3)
-            api_dev.append(st.ms_total)
-    # accuracy against the FP64 power series of the same walk semantics
-    mu = G.expected_visits(p, src)
-    est = c / B
-    l1 = float(np.abs(est - mu).sum())
-    bound = float(np.sqrt(L * mu / B).sum())
-    exact_top = set(np.argsort(-mu, kind="stable")[:100].tolist())
-    overlap = len(exact_top & set(ids[0].tolist()))
-    top_from_counts = np.lexsort((np.arange(nv), -c))[:100]
-    top_from_counts = np.where(c[top_from_counts] > 0, top_from_counts, 0xFFFFFFFF)
-    line = {"metric": "walk-steps/s", "value": steps / (ms * 1e-3), "unit": "walk-steps/s", "workload": "ppr1",
-            "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": f"single-source PPR, R-MAT scale {scale} ef {args.edge_factor}, {B} walks from "
-                                   f"the generator's vertex 0 (id {src} after permutation, the top out-degree "
-                                   f"vertex), stop p=0.15, dangling->source, L<=20", "walk_steps": steps},
-            "queries_per_s": 1e3 / ms,
-            "ppr_api": {"device_ms": statistics.median(api_dev), "wall_ms": statistics.median(api_wall),
-                        "what": "gw_ppr_run, one query of the same walks, batch tag + walk + top-100, warm"},
-            "accuracy": {"l1_error": l1, "mc_bound_l1": bound, "top100_overlap_with_fp64": overlap,
-                         "top100_api_equals_counts": bool(np.array_equal(ids[0], top_from_counts))}}
-    G.close()
+    try:
+        nv = G.nv
+        # "vertex 0" of the R-MAT generator (all-zero quadrant bits: its hub) is
+        # the vertex with the largest out-degree once ids are permuted
+        rp, _ = G.export_csr()
+        src = int(np.argmax(np.diff(rp.astype(np.int64))))
+        del rp
+        j = torch.arange(B, dtype=torch.int64, device="cuda")
+        walks = torch.stack([torch.full_like(j, src), j, torch.full_like(j, src), torch.zeros_like(j)], 1)
+        walks = walks.to(torch.int32).contiguous()
+        counts = torch.zeros(nv, dtype=torch.int32, device="cuda")
+        p = gw.params(gw.RULE_PPR, gw.SINK_VERTEX_COUNT, L, seed=args.walk_seed, aggregate=True)
+        sh = torch.cuda.current_stream().cuda_stream
+        for _ in range(max(3, args.warmup)):
+            counts.zero_()
+            G.walk_device(p, walks, B, counts=counts, stream=sh)
+        G.sync(sh)
+        steps = max(1, args.steps)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a, b in ev:
+            counts.zero_()
+            a.record()
+            G.walk_device(p, walks, B, counts=counts, stream=sh)
+            b.record()
+        G.sync(sh)
+        ms = statistics.median(a.elapsed_time(b) for a, b in ev)
+        c = counts.cpu().numpy().view(np.uint32).copy()
+        nsteps = int(c.astype(np.int64).sum())
+        # the same query through the C ABI (gw_ppr_run, host arrays in and out): warm calls
+        api_dev, api_wall = [], []
+        for i in range(3 + steps):
+            t0 = time.perf_counter()
+            ids, cnt, st = G.ppr(p, np.array([src], np.uint32), np.array([B], np.uint32), k=100)
+            if i >= 3:
+                api_wall.append((time.perf_counter() - t0) * 1e3)
+                api_dev.append(st.ms_total)
+        mu = G.expected_visits(p, src)
+        acc = accuracy.measured_accuracy(mu, B, L, ids[0], counts=c, k=100)
+        top_from_counts = accuracy.count_topk(np.arange(nv), c, 100)
+        acc["top100_api_equals_counts"] = bool(np.array_equal(ids[0][ids[0] != 0xFFFFFFFF], top_from_counts))
+        return {"metric": "walk-steps/s", "value": nsteps / (ms * 1e-3), "unit": "walk-steps/s", "workload": "ppr1",
+                "n_gpus": 1, "steps": steps, "warmup": max(3, args.warmup), "ms_per_step": ms,
+                "higher_is_better": True, "dtype": "u32", "data": "synthetic",
+                "config": {"workload": f"single-source PPR, R-MAT scale {scale} ef {args.edge_factor}, {B} walks "
+                                       f"from the generator's vertex 0 (id {src} after permutation, the top "
+                                       f"out-degree vertex), stop p=0.15, dangling->source, L<=20",
+                           "walk_steps": nsteps},
+                "queries_per_s": 1e3 / ms,
+                "ppr_api": {"device_ms": statistics.median(api_dev), "wall_ms": statistics.median(api_wall),
+                            "what": "gw_ppr_run, one query of the same walks, batch tag + walk + top-100, warm"},
+                "accuracy_vs_fp64": acc, "gpu_launches": steps}
+    finally:
+        G.close()
+
+
+def ppr1_arm(args) -> None:
+    line = ppr1_measure(args)
+    line["scaling"], line["vs_baseline"] = "weak", None
     print(json.dumps(line), flush=True)
 
 

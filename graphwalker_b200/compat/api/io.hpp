@@ -1,5 +1,15 @@
 // Drop-in GraphWalker API: full-length pread/pwrite helpers
 // (the reference's src/api/io.hpp:11-76).
+//
+// Two deliberate differences in writefile / appendfile:
+//  * they write (bufptr - buf) * sizeof(T) bytes, the whole buffer.  The
+//    reference passes the element count bufptr - buf as the byte count
+//    (io.hpp:62,74), so for sizeof(T) > 1 it writes only the first
+//    1/sizeof(T) of the buffer;
+//  * writefile opens with O_TRUNC.  The reference opens without it
+//    (io.hpp:57), so a shorter write leaves the old file's tail in place.
+// No path of this engine reads files written by these helpers; they exist so
+// that programs calling them compile, and they write what the call names.
 #ifndef DEF_IOUTIL_HPP
 #define DEF_IOUTIL_HPP
 

@@ -10,6 +10,9 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 /* ------------------------------------------------------------------------ */
 /* Philox4x32-10, from the round function and constants published in        */
@@ -142,6 +145,10 @@ uint32_t gwo_run_walks(const uint64_t *rowptr, const uint32_t *colidx, uint32_t 
                        uint64_t *closure, uint32_t *final_cur, uint32_t *final_hop) {
     uint32_t status = 0;
     uint32_t thr = gwo_continue_threshold(p->jump_prob);
+    /* Walks are independent (every draw is keyed on the walk's id and hop),
+     * so they run on all host threads; the shared sinks are updated
+     * atomically, which leaves every count equal to the sequential loop's. */
+#pragma omp parallel for schedule(dynamic, 4096) reduction(| : status)
     for (uint64_t i = 0; i < nwalks; ++i) {
         uint32_t v = cur[i], h = hop0[i], s = src[i], wid = id[i];
         uint32_t k = 0;
@@ -150,12 +157,18 @@ uint32_t gwo_run_walks(const uint64_t *rowptr, const uint32_t *colidx, uint32_t 
             if (p->rule == GWO_RULE_PROB && h >= p->max_hops) { status |= GWO_ST_HOP_OVF; break; }
             if (v >= nv) { status |= GWO_ST_BOUNDS; break; }
             /* updateInfo(sourId, dstId, threadid, hop) precedes the draws */
-            if (counts) counts[v] += 1;
+            if (counts) {
+#pragma omp atomic
+                counts[v] += 1;
+            }
             if (paths) {
                 if (k < stride) paths[i * (uint64_t)stride + k] = v;
                 else status |= GWO_ST_PATH_OVF;
             }
-            if (closure && (int64_t)h >= (int64_t)p->L - 1 && v == s) *closure += 1; /* graphlet.cpp:46-52 */
+            if (closure && (int64_t)h >= (int64_t)p->L - 1 && v == s) { /* graphlet.cpp:46-52 */
+#pragma omp atomic
+                *closure += 1;
+            }
             k++;
             if (!hop_advance(rowptr, colidx, p, thr, wid, s, h, &v)) break;
             h++;
@@ -292,17 +305,43 @@ void gwo_rmat_edge(uint64_t e, uint32_t scale, uint64_t seed,
     *dst = gwo_rmat_permute(d, scale, seed);
 }
 
+/* LSD radix sort of 64-bit keys, 16 bits per pass.  Each thread counts and
+ * scatters one contiguous chunk; the per-(digit, thread) offsets keep every
+ * pass stable, so the result is the sequential sort's. */
 static void radix_sort_u64(uint64_t *a, uint64_t *tmp, uint64_t n) {
-    size_t *cnt = (size_t *)malloc(65536 * sizeof(size_t));
+    int nt = 1;
+#ifdef _OPENMP
+    nt = omp_get_max_threads();
+#endif
+    size_t *cnt = (size_t *)malloc((size_t)65536 * nt * sizeof(size_t));
     for (int pass = 0; pass < 4; ++pass) {
         int shift = pass * 16;
-        memset(cnt, 0, 65536 * sizeof(size_t));
-        for (uint64_t i = 0; i < n; ++i) cnt[(a[i] >> shift) & 0xffff]++;
-        size_t sum = 0;
-        for (int b = 0; b < 65536; ++b) { size_t c = cnt[b]; cnt[b] = sum; sum += c; }
-        for (uint64_t i = 0; i < n; ++i) tmp[cnt[(a[i] >> shift) & 0xffff]++] = a[i];
-        memcpy(a, tmp, n * sizeof(uint64_t));
+#pragma omp parallel num_threads(nt)
+        {
+            int t = 0;
+#ifdef _OPENMP
+            t = omp_get_thread_num();
+#endif
+            uint64_t lo = n * (uint64_t)t / nt, hi = n * (uint64_t)(t + 1) / nt;
+            size_t *c = cnt + (size_t)65536 * t;
+            memset(c, 0, 65536 * sizeof(size_t));
+            for (uint64_t i = lo; i < hi; ++i) c[(a[i] >> shift) & 0xffff]++;
+#pragma omp barrier
+#pragma omp single
+            {
+                size_t sum = 0;
+                for (int b = 0; b < 65536; ++b)
+                    for (int u = 0; u < nt; ++u) {
+                        size_t x = cnt[(size_t)65536 * u + b];
+                        cnt[(size_t)65536 * u + b] = sum;
+                        sum += x;
+                    }
+            }
+            for (uint64_t i = lo; i < hi; ++i) tmp[c[(a[i] >> shift) & 0xffff]++] = a[i];
+        }
+        uint64_t *sw = a; a = tmp; tmp = sw;
     }
+    /* four passes: the sorted keys are back in the caller's array */
     free(cnt);
 }
 
@@ -312,19 +351,22 @@ uint64_t gwo_rmat_csr(uint32_t scale, uint64_t nedges_raw, uint64_t seed,
     uint64_t nv = 1ull << scale;
     uint64_t *keys = (uint64_t *)malloc((nedges_raw ? nedges_raw : 1) * sizeof(uint64_t));
     uint64_t *tmp = (uint64_t *)malloc((nedges_raw ? nedges_raw : 1) * sizeof(uint64_t));
-    uint64_t m = 0;
+    /* edges are generated independently (Philox keyed on the edge index);
+     * self-loops (dropped, conversions.hpp:237) become all-ones keys that
+     * sort behind every real edge */
+#pragma omp parallel for schedule(static)
     for (uint64_t e = 0; e < nedges_raw; ++e) {
         uint32_t s, d;
         gwo_rmat_edge(e, scale, seed, ta, tab, tabc, &s, &d);
-        if (s == d) continue; /* self-loops dropped (conversions.hpp:237) */
-        keys[m++] = ((uint64_t)s << 32) | d;
+        keys[e] = s == d ? ~0ull : ((uint64_t)s << 32) | d;
     }
-    radix_sort_u64(keys, tmp, m);
+    radix_sort_u64(keys, tmp, nedges_raw);
+    uint64_t m = nedges_raw;
+    while (m > 0 && keys[m - 1] == ~0ull) --m;
     memset(rowptr, 0, (nv + 1) * sizeof(uint64_t));
-    for (uint64_t i = 0; i < m; ++i) {
-        rowptr[(keys[i] >> 32) + 1]++;
-        colidx[i] = (uint32_t)keys[i];
-    }
+    for (uint64_t i = 0; i < m; ++i) rowptr[(keys[i] >> 32) + 1]++;
+#pragma omp parallel for schedule(static)
+    for (uint64_t i = 0; i < m; ++i) colidx[i] = (uint32_t)keys[i];
     for (uint64_t v = 0; v < nv; ++v) rowptr[v + 1] += rowptr[v];
     free(keys);
     free(tmp);

@@ -1,9 +1,11 @@
 /*
  * gw_oracle.h -- TEST INFRASTRUCTURE ONLY.
  *
- * A plain-C, single-threaded restatement of GraphWalker's random-walk hot
- * path, used by tests/, __graft_entry__.smoke() and bench.py's cpu_baseline
- * leg as the checker.  Nothing in graphwalker_b200/ links, loads or calls
+ * A plain-C restatement of GraphWalker's random-walk hot path.  Its results
+ * are those of a sequential loop; the loops over independent items (walks,
+ * generated edges) run on the host's threads with OpenMP so that the
+ * configs' full sizes can be checked in seconds.  It is used by tests/,
+ * __graft_entry__.smoke() and bench.py's cpu_baseline leg as the checker.  Nothing in graphwalker_b200/ links, loads or calls
  * this code; the product path is the CUDA library only.
  *
  * Parity pin: the restatement is checked against golden vectors produced by

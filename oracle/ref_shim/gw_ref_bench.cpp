@@ -21,7 +21,14 @@
  * Usage: gw_ref_bench <graph base> <blocksize_kb> <N> <L> <stride> <warmup>
  *                     <steps> <execthreads> [rwd | msppr <firstsource>
  *                     <numsources> <walkspersource>]
- * Prints one line per timed run: "step <i> walks <n> steps <visits> sec <t>".
+ * Prints one line per timed run:
+ *   "step <i> walks <n> steps <visits> sec <t> threads_after <k>"
+ * threads_after is omp_get_max_threads() when the run returns.  The engine's
+ * exec_updates sets the OpenMP thread count to 1 for a block with fewer than
+ * 100 walks and never restores it (graphwalker.hpp:260), so k == 1 with
+ * execthreads > 1 means that fallback fired during the run and the rest of
+ * the run was single-threaded.  Each run starts again at execthreads (the
+ * apps' startWalksbyApp calls omp_set_num_threads, as the reference's apps do).
  */
 #include <chrono>
 #include <cmath>
@@ -140,8 +147,9 @@ int main(int argc, const char **argv) {
             engine.run(prog, 0.2f);
             auto t1 = std::chrono::steady_clock::now();
             if (i >= warmup)
-                printf("step %d walks %llu steps %llu sec %.6f\n", i - warmup, (unsigned long long)prog.started,
-                       prog.total_visits(), std::chrono::duration<double>(t1 - t0).count());
+                printf("step %d walks %llu steps %llu sec %.6f threads_after %d\n", i - warmup,
+                       (unsigned long long)prog.started, prog.total_visits(),
+                       std::chrono::duration<double>(t1 - t0).count(), omp_get_max_threads());
             fflush(stdout);
         }
         return 0;
@@ -158,8 +166,9 @@ int main(int argc, const char **argv) {
         unsigned long long visits = 0;
         for (vid_t v = 0; v < N; ++v) visits += prog.vertex_value[v];
         if (i >= warmup)
-            printf("step %d walks %llu steps %llu sec %.6f\n", i - warmup, (unsigned long long)prog.started,
-                   visits, std::chrono::duration<double>(t1 - t0).count());
+            printf("step %d walks %llu steps %llu sec %.6f threads_after %d\n", i - warmup,
+                   (unsigned long long)prog.started, visits, std::chrono::duration<double>(t1 - t0).count(),
+                   omp_get_max_threads());
         fflush(stdout);
     }
     return 0;

@@ -13,10 +13,11 @@ import numpy as np
 import pytest
 
 from conftest import ROOT, golden_runs, load_golden
+from oracle.refpath import REFERENCE
 
 COMPAT = ROOT / "graphwalker_b200" / "compat"
 APPS_DIR = COMPAT / "_apps"
-REFERENCE_APPS = Path("/root/reference/apps")
+REFERENCE_APPS = REFERENCE / "apps"
 LIVE_APPS = ["rwdomination", "rawrandomwalks", "msppr", "kk_ppr", "graphlet", "simrank"]
 
 

@@ -101,5 +101,5 @@ def test_server_open_fails_cleanly_without_memory(cuda_device):
         gw.inject_fault(gw.FAULT_NONE)
         with G.serve(p, table_slots=1 << 16) as S:
             t = S.submit(5, 200)
-            ids, counts, _ = S.wait(t)
+            ids, counts, _ = S.wait(t, 60_000)
             assert counts[0] >= 200  # the source is visited by every walk

@@ -9,6 +9,10 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
+# every wait is bounded: a scheduler thread that died fails the test with
+# GW_E_TIMEOUT instead of hanging it
+WAIT_MS = 60_000
+
 
 @pytest.fixture(scope="module")
 def graph(cuda_device):
@@ -33,14 +37,14 @@ def test_result_is_the_same_alone_and_in_a_mix(graph):
     src, bud = _queries(graph, 200, 1)
     x_src, x_bud, x_stream = int(src[0]), 20000, 777
     with graph.serve(p, quantum=4096) as S:
-        alone = S.wait(S.submit(x_src, x_bud, x_stream))
+        alone = S.wait(S.submit(x_src, x_bud, x_stream), WAIT_MS)
     with graph.serve(p, quantum=4096) as S:
         tickets = [S.submit(int(s), int(b), i) for i, (s, b) in enumerate(zip(src[:100], bud[:100]))]
         tx = S.submit(x_src, x_bud, x_stream)
         tickets += [S.submit(int(s), int(b), 1000 + i) for i, (s, b) in enumerate(zip(src[100:], bud[100:]))]
-        mixed = S.wait(tx)
+        mixed = S.wait(tx, WAIT_MS)
         for t in tickets:
-            S.wait(t)
+            S.wait(t, WAIT_MS)
         st = S.stats()
     assert np.array_equal(alone[0], mixed[0]) and np.array_equal(alone[1], mixed[1])
     assert st.completed == 201 and st.supersteps < 201  # queries shared supersteps
@@ -55,7 +59,7 @@ def test_served_stream_zero_equals_batch_api_and_plain_server(graph):
     for mode in (gw._lib.SERVE_BATCHED, gw._lib.SERVE_PLAIN):
         with graph.serve(p, mode=mode) as S:
             tickets = [S.submit(int(s), int(b), 0) for s, b in zip(src, bud)]
-            res[mode] = [S.wait(t)[:2] for t in tickets]
+            res[mode] = [S.wait(t, WAIT_MS)[:2] for t in tickets]
     for q in range(30):
         ids, cnt, _ = graph.ppr(p, src[q:q + 1], bud[q:q + 1], k=100)
         for mode in res:
@@ -68,11 +72,11 @@ def test_table_restarts_and_arena_admission(graph):
     p = gw.params(gw.RULE_JUMP, gw.SINK_NONE, 20, seed=5)
     src, bud = _queries(graph, 40, 3, max_budget=3000)
     with graph.serve(p) as S:
-        ref = [S.wait(S.submit(int(s), int(b), 9))[:2] for s, b in zip(src, bud)]
+        ref = [S.wait(S.submit(int(s), int(b), 9), WAIT_MS)[:2] for s, b in zip(src, bud)]
     p.table_factor = 1  # tables fill up: restarts with larger tables
     with graph.serve(p, table_slots=1 << 18) as S:  # a small arena: queries queue for space
         tickets = [S.submit(int(s), int(b), 9) for s, b in zip(src, bud)]
-        got = [S.wait(t) for t in tickets]
+        got = [S.wait(t, WAIT_MS) for t in tickets]
         assert S.stats().restarts > 0
         with pytest.raises(GwError) as e:
             S.submit(int(src[0]), 1 << 20, 1)  # needs more slots than the arena has
@@ -89,6 +93,6 @@ def test_scheduled_arrivals_and_latency_accounting(graph):
         t0 = S.clock_ns() + 2_000_000
         arrivals = t0 + np.cumsum(np.random.default_rng(0).exponential(1e9 / 20000, 300)).astype(np.int64)
         tickets = [S.submit(int(s), int(b), i, int(a)) for i, (s, b, a) in enumerate(zip(src, bud, arrivals))]
-        timings = [S.wait(t)[2] for t in tickets]
+        timings = [S.wait(t, WAIT_MS)[2] for t in tickets]
     for a, tm in zip(arrivals, timings):
         assert tm.arrival_ns == a and tm.admit_ns >= a and tm.done_ns > tm.admit_ns
