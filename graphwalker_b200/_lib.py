@@ -21,6 +21,7 @@ GW_E_BOUNDS, GW_E_OVERFLOW, GW_E_STATE, GW_E_TIMEOUT = 5, 6, 7, 8
 RULE_JUMP, RULE_STOP, RULE_PROB, RULE_RESTART, RULE_PPR = 0, 1, 2, 3, 4
 SINK_NONE, SINK_VERTEX_COUNT, SINK_PATH_RECORD, SINK_CLOSURE_COUNT = 0, 1, 2, 3
 MODE_RESIDENT, MODE_BLOCKED = 0, 1
+RNG_PHILOX, RNG_NATIVE = 0, 1
 RESIDENT_HBM, STREAM_PINNED = 0, 1
 
 
@@ -34,7 +35,7 @@ class WalkParams(Structure):
                 ("path_stride", c_uint32), ("max_hops", c_uint32), ("prob", c_float),
                 ("aggregate", c_uint32), ("max_supersteps", c_uint32), ("cache_hints", c_uint32),
                 ("table_factor", c_uint32), ("block_lo", c_uint32), ("block_hi", c_uint32),
-                ("reserved", c_uint32 * 2)]
+                ("rng", c_uint32), ("reserved", c_uint32)]
 
 
 SERVE_BATCHED, SERVE_PLAIN = 0, 1

@@ -117,6 +117,13 @@ class graphwalker_engine {
     p.seed = get_option_long("seed", 42);
     p.prob = prob;
     p.mode = get_option_string("gw_mode", "resident") == "blocked" ? GW_MODE_BLOCKED : GW_MODE_RESIDENT;
+    // gw_rng philox (default): the deterministic mode, bit-exact to the
+    // reference engine with its rand_r routed to the same Philox stream;
+    // gw_rng native: one Philox block per two hops (checked statistically)
+    const std::string rng = get_option_string("gw_rng", "philox");
+    if (rng != "philox" && rng != "native")
+      logstream(LOG_FATAL) << "gw_rng must be philox or native, not " << rng << std::endl;
+    p.rng = rng == "native" ? GW_RNG_NATIVE : GW_RNG_PHILOX;
     const bool by_source = get_option_string("gw_walk_id", "index") == "source";
     const bool count_sink = get_option_string("gw_sink", "replay") == "count";
 

@@ -130,7 +130,7 @@ gw_status install_graph(gw_ctx* ctx, const uint64_t* rowptr, const uint32_t* col
   } else {
     GW_CUDA(ctx, ctx->d_rowptr.ensure(rp_bytes), "rowptr alloc");
     GW_CUDA(ctx, ctx->d_colidx.ensure(ci_bytes), "colidx alloc");
-    GW_CUDA(ctx, ctx->d_vrec.ensure((size_t)nv * sizeof(uint64_t)), "vrec alloc");
+    GW_CUDA(ctx, ctx->d_vrec.ensure(gw::vrec_bytes(nv)), "vrec alloc");
     GW_CUDA(ctx, cudaMemcpyAsync(ctx->d_rowptr.p, rowptr, rp_bytes, cudaMemcpyHostToDevice,
                                  ctx->stream), "rowptr copy");
     GW_CUDA(ctx, cudaMemcpyAsync(ctx->d_colidx.p, colidx, ci_bytes, cudaMemcpyHostToDevice,
@@ -185,6 +185,8 @@ gw_status make_walk_args(gw_ctx* ctx, const gw_walk_params* p, WalkArgs* a) {
   a->path_stride = p->path_stride;
   a->lo = 0;
   a->hi = ctx->nv;
+  if (p->rng > GW_RNG_NATIVE) return ctx->fail(GW_E_INVALID, "unknown rng %u", p->rng);
+  a->native = p->rng == GW_RNG_NATIVE ? 1u : 0u;
   return GW_OK;
 }
 
@@ -440,7 +442,7 @@ gw_status gw_open_rmat(uint32_t scale, uint32_t edge_factor, uint64_t seed, doub
     cudaError_t e = ctx->d_blocks.ensure(cnt * sizeof(uint32_t));
     if (e == cudaSuccess)
       e = cudaMemcpy(ctx->d_blocks.p, blocks.data(), cnt * sizeof(uint32_t), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = ctx->d_vrec.ensure((size_t)nv * 8);
+    if (e == cudaSuccess) e = ctx->d_vrec.ensure(gw::vrec_bytes(nv));
     if (e == cudaSuccess)
       e = gw::launch_build_vrec(rowptr, nv, ctx->d_vrec.as<unsigned long long>(), ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -532,7 +534,7 @@ gw_status gw_set_residency(gw_ctx* ctx, uint32_t residency, uint32_t nmblocks) {
   } else {
     GW_CUDA(ctx, ctx->d_rowptr.ensure(rp), "rowptr alloc");
     GW_CUDA(ctx, ctx->d_colidx.ensure(ci), "colidx alloc");
-    GW_CUDA(ctx, ctx->d_vrec.ensure((size_t)ctx->nv * 8), "vrec alloc");
+    GW_CUDA(ctx, ctx->d_vrec.ensure(gw::vrec_bytes(ctx->nv)), "vrec alloc");
     GW_CUDA(ctx, cudaMemcpy(ctx->d_rowptr.p, ctx->h_rowptr.p, rp, cudaMemcpyHostToDevice), "rowptr to device");
     if (ci) GW_CUDA(ctx, cudaMemcpy(ctx->d_colidx.p, ctx->h_colidx.p, ci, cudaMemcpyHostToDevice), "colidx to device");
     GW_CUDA(ctx, gw::launch_build_vrec(ctx->d_rowptr.as<unsigned long long>(), ctx->nv,

@@ -156,6 +156,7 @@ struct gw_ctx {
     g.rowptr = d_rowptr.as<const unsigned long long>();
     g.colidx = d_colidx.as<const uint32_t>();
     g.erec = d_erec.p && d_erec.bytes >= ne * sizeof(ulonglong2) ? d_erec.as<const ulonglong2>() : nullptr;
+    g.out_bits = d_vrec.p && d_vrec.bytes >= gw::vrec_bytes(nv) ? reinterpret_cast<const uint32_t*>(g.vrec + nv) : nullptr;
     g.nv = nv;
     return g;
   }

@@ -103,6 +103,7 @@ struct WalkArgs {
   uint32_t seed_lo, seed_hi;
   uint32_t path_stride;
   uint32_t lo, hi;     // block range [lo, hi) in blocked mode
+  uint32_t native;     // 1 = native-RNG mode (one Philox block per two hops)
 };
 
 struct GraphView {
@@ -113,6 +114,9 @@ struct GraphView {
   // of the edge's target, y = the target's id.  Moving along an edge then
   // reads the next vertex and its record in one 16-byte load.
   const ulonglong2* __restrict__ erec;
+  // Out-edge bitmap (nv bits, stored right after the packed records; NULL
+  // when the records are not built): bit v is set when v has out-edges.
+  const uint32_t* __restrict__ out_bits;
   uint32_t nv;
 };
 
@@ -132,7 +136,7 @@ __device__ __forceinline__ constexpr bool rule_capped() {
 // walk ends inside this hop (stop rules); otherwise v is the next vertex and
 // the caller increments the hop.  Loads go through the read-only path.
 struct L2Hints {
-  uint64_t rec, col, cnt;
+  uint64_t rec, col, cnt, bits;
 };
 
 __device__ __forceinline__ L2Hints make_hints(uint32_t flags) {
@@ -140,18 +144,61 @@ __device__ __forceinline__ L2Hints make_hints(uint32_t flags) {
   h.rec = l2_policy(false, flags & kHintRecordsEvictLast);
   h.col = l2_policy(flags & kHintColumnsEvictFirst, false);
   h.cnt = l2_policy(false, flags & kHintCountsEvictLast);
+  h.bits = l2_policy(false, true);  // the out-edge bitmap is small and read at every jump
   return h;
+}
+
+// ---- per-hop draws ----
+// Philox mode (GW_RNG_PHILOX, the deterministic mode): the hop's two draws
+// are words 0 and 1 of Philox(key = seed, counter = (id, hop, stream, 0)),
+// consumed in the reference's order, so trajectories equal the shimmed
+// reference's.  Native-RNG mode (GW_RNG_NATIVE): one Philox block serves two
+// hops -- words 0, 1 for the even hop 2m and words 2, 3 for hop 2m + 1 of
+// Philox(seed, (id, m, stream, kNativeTag)) -- so a walk computes one block
+// per two hops.  Its draws are still a pure function of (seed, id, hop,
+// stream), independent of the schedule; the mode is checked statistically
+// against the FP64 power series, not against the reference's trajectories.
+constexpr uint32_t kNativeTag = 0x4E415456u;  // "NATV"
+constexpr uint32_t kNoHop = 0xffffffffu;
+
+// The spare words of the last native block a thread computed, valid for
+// hop `hop` of the walk the thread holds; reset whenever it takes a walk.
+struct DrawCache {
+  uint32_t z, w, hop;
+  __device__ __forceinline__ void reset() { hop = kNoHop; }
+};
+
+struct Draws {
+  uint32_t d0, d1;
+};
+
+__device__ __forceinline__ Draws hop_draws(const WalkArgs& a, uint32_t id, uint32_t hop, uint32_t stream,
+                                           DrawCache& dc) {
+  if (!a.native) {
+    const Philox4 ph = philox4x32_10(id, hop, stream, 0u, a.seed_lo, a.seed_hi);
+    return Draws{ph.x >> 1, ph.y >> 1};
+  }
+  if (dc.hop == hop) {
+    dc.hop = kNoHop;
+    return Draws{dc.z >> 1, dc.w >> 1};
+  }
+  const Philox4 ph = philox4x32_10(id, hop >> 1, stream, kNativeTag, a.seed_lo, a.seed_hi);
+  if (hop & 1u) return Draws{ph.z >> 1, ph.w >> 1};
+  dc.z = ph.z;
+  dc.w = ph.w;
+  dc.hop = hop + 1;
+  return Draws{ph.x >> 1, ph.y >> 1};
 }
 
 template <int RULE>
 __device__ __forceinline__ bool hop_advance_rec(const GraphView& g, const WalkArgs& a, const L2Hints& hp,
                                                 uint32_t id, uint32_t src, uint32_t hop, uint32_t& v,
-                                                unsigned long long rec, uint32_t stream = 0u);
+                                                unsigned long long rec, DrawCache& dc, uint32_t stream = 0u);
 
 template <int RULE>
 __device__ __forceinline__ bool hop_advance(const GraphView& g, const WalkArgs& a, const L2Hints& hp,
-                                            uint32_t id, uint32_t src, uint32_t hop, uint32_t& v) {
-  return hop_advance_rec<RULE>(g, a, hp, id, src, hop, v, ld_nc_u64(g.vrec + v, hp.rec));
+                                            uint32_t id, uint32_t src, uint32_t hop, uint32_t& v, DrawCache& dc) {
+  return hop_advance_rec<RULE>(g, a, hp, id, src, hop, v, ld_nc_u64(g.vrec + v, hp.rec), dc);
 }
 
 // The hop with v's packed record already loaded (callers that have other
@@ -161,10 +208,10 @@ __device__ __forceinline__ bool hop_advance(const GraphView& g, const WalkArgs& 
 template <int RULE>
 __device__ __forceinline__ bool hop_advance_rec(const GraphView& g, const WalkArgs& a, const L2Hints& hp,
                                                 uint32_t id, uint32_t src, uint32_t hop, uint32_t& v,
-                                                unsigned long long rec, uint32_t stream) {
-  const Philox4 ph = philox4x32_10(id, hop, stream, 0u, a.seed_lo, a.seed_hi);
-  const uint32_t d0 = ph.x >> 1;
-  const uint32_t d1 = ph.y >> 1;
+                                                unsigned long long rec, DrawCache& dc, uint32_t stream) {
+  const Draws dr = hop_draws(a, id, hop, stream, dc);
+  const uint32_t d0 = dr.d0;
+  const uint32_t d1 = dr.d1;
   unsigned long long off = rec >> kDegBits;
   unsigned long long deg = rec & kDegEscape;
   if (deg == kDegEscape) {  // mega-hub: exact degree from the row pointer
@@ -202,6 +249,17 @@ __device__ __forceinline__ unsigned long long vertex_rec(const GraphView& g, con
   return v < g.nv ? ld_nc_u64(g.vrec + v, hp.rec) : 0ull;
 }
 
+// The record of a jump target.  A target without out-edges needs none: its
+// next hop reads only the degree, which is 0 (its record's offset field is
+// never used), so the 8-byte record load -- a DRAM miss for most uniformly
+// drawn targets -- is replaced by a read of the out-edge bitmap, which stays
+// in L2.  Targets with out-edges load their record as before.
+__device__ __forceinline__ unsigned long long jump_rec(const GraphView& g, const L2Hints& hp, uint32_t v) {
+  if (v >= g.nv) return 0ull;
+  if (g.out_bits && !((ld_nc_u32(g.out_bits + (v >> 5), hp.bits) >> (v & 31u)) & 1u)) return 0ull;
+  return ld_nc_u64(g.vrec + v, hp.rec);
+}
+
 // The same hop over the edge-record layout: the record of v is carried in
 // `rec` from the previous hop.  Moving along an edge reads the next vertex and
 // its record together; a jump reads the record of its target; a return to the
@@ -210,10 +268,10 @@ template <int RULE>
 __device__ __forceinline__ bool hop_advance_carried(const GraphView& g, const WalkArgs& a, const L2Hints& hp,
                                                     uint32_t id, uint32_t src, unsigned long long src_rec,
                                                     uint32_t hop, uint32_t& v, unsigned long long& rec,
-                                                    uint32_t stream = 0u) {
-  const Philox4 ph = philox4x32_10(id, hop, stream, 0u, a.seed_lo, a.seed_hi);
-  const uint32_t d0 = ph.x >> 1;
-  const uint32_t d1 = ph.y >> 1;
+                                                    DrawCache& dc, uint32_t stream = 0u) {
+  const Draws dr = hop_draws(a, id, hop, stream, dc);
+  const uint32_t d0 = dr.d0;
+  const uint32_t d1 = dr.d1;
   unsigned long long off = rec >> kDegBits;
   unsigned long long deg = rec & kDegEscape;
   if (deg == kDegEscape) {  // mega-hub: exact degree from the row pointer
@@ -232,7 +290,7 @@ __device__ __forceinline__ bool hop_advance_carried(const GraphView& g, const Wa
   const uint32_t dj = deg > 0 ? d1 : d0;
   if (RULE == GW_RULE_JUMP) {
     v = dj % a.njump;
-    rec = vertex_rec(g, hp, v);
+    rec = jump_rec(g, hp, v);
     return true;
   } else if (RULE == GW_RULE_RESTART) {
     v = src;
@@ -263,14 +321,14 @@ template <int RULE>
 __device__ __forceinline__ bool hop_advance_slice(const unsigned long long* __restrict__ beg_pos,
                                                   const uint32_t* __restrict__ csr,
                                                   const WalkArgs& a, uint32_t id, uint32_t src,
-                                                  uint32_t hop, uint32_t& v) {
+                                                  uint32_t hop, uint32_t& v, DrawCache& dc) {
   const uint32_t vl = v - a.lo;
   const unsigned long long b0 = __ldg(beg_pos);
   const unsigned long long b = __ldg(beg_pos + vl);
   const unsigned long long deg = __ldg(beg_pos + vl + 1) - b;
-  const Philox4 ph = philox4x32_10(id, hop, 0u, 0u, a.seed_lo, a.seed_hi);
-  const uint32_t d0 = ph.x >> 1;
-  const uint32_t d1 = ph.y >> 1;
+  const Draws dr = hop_draws(a, id, hop, 0u, dc);
+  const uint32_t d0 = dr.d0;
+  const uint32_t d1 = dr.d1;
   if (deg > 0 && d0 >= a.thr) {
     const unsigned long long r =
         deg > 0x7fffffffull ? (unsigned long long)d1 : (unsigned long long)(d1 % (uint32_t)deg);

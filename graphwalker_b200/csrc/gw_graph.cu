@@ -25,6 +25,20 @@ __global__ void build_vrec_kernel(const unsigned long long* __restrict__ rowptr,
   }
 }
 
+// Out-edge bitmap: word w holds the bits of vertices 32w .. 32w + 31.
+__global__ void build_out_bits_kernel(const unsigned long long* __restrict__ rowptr, uint32_t nv,
+                                      uint32_t* __restrict__ bits) {
+  const uint64_t nw = ((uint64_t)nv + 31) / 32;
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw;
+       w += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t x = 0;
+    const uint64_t v0 = w * 32;
+    for (uint32_t j = 0; j < 32 && v0 + j < nv; ++j)
+      x |= (rowptr[v0 + j + 1] > rowptr[v0 + j] ? 1u : 0u) << j;
+    bits[w] = x;
+  }
+}
+
 struct RmatArgs {
   uint32_t scale, mask, half;
   uint32_t key0, key1;
@@ -117,6 +131,8 @@ cudaError_t launch_build_vrec(const unsigned long long* rowptr, uint32_t nv,
                               unsigned long long* vrec, cudaStream_t stream) {
   if (nv == 0) return cudaSuccess;
   build_vrec_kernel<<<grid_for(nv), 256, 0, stream>>>(rowptr, nv, vrec);
+  build_out_bits_kernel<<<grid_for((nv + 31) / 32), 256, 0, stream>>>(rowptr, nv,
+                                                                      reinterpret_cast<uint32_t*>(vrec + nv));
   return cudaGetLastError();
 }
 

@@ -63,6 +63,10 @@ cudaError_t launch_build_erec(const uint32_t* colidx, const unsigned long long* 
                               ulonglong2* erec, cudaStream_t stream);
 
 // ---- graph kernels (gw_graph.cu) ----
+// Bytes of the vertex-record buffer: nv packed records, then the out-edge
+// bitmap (one bit per vertex, in 32-bit words).
+inline size_t vrec_bytes(uint32_t nv) { return (size_t)nv * 8 + (((size_t)nv + 31) / 32) * 4; }
+// Fills the packed records and the out-edge bitmap (vrec_bytes(nv) bytes at vrec).
 cudaError_t launch_build_vrec(const unsigned long long* rowptr, uint32_t nv,
                               unsigned long long* vrec, cudaStream_t stream);
 // rowptr[nv + 1] and colidx[n] of edge keys (source << 32 | target) sorted by

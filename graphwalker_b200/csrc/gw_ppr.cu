@@ -143,6 +143,8 @@ __global__ void __launch_bounds__(kPprThreads)
   unsigned long long j = 0, id_shift = 0, q_lo = 1, q_hi = 0;
   unsigned long long cur_rec = 0, src_rec = 0;  // edge-record mode: records of v and of the source
   uint32_t q = 0, src = 0, sid = 0, v = 0, hop = 0, st = 0, nvisit = 0;
+  DrawCache dc;
+  dc.reset();
   for (;;) {
     // Idle lanes take the next walks of the warp's chunk, in lane order.
     uint32_t idle = __ballot_sync(~0u, !busy);
@@ -180,6 +182,7 @@ __global__ void __launch_bounds__(kPprThreads)
         v = src;
         cur_rec = src_rec;
         hop = 0;
+        dc.reset();
       }
       const uint32_t n_idle = __popc(idle);
       c_next += n_idle < avail ? n_idle : avail;
@@ -220,8 +223,8 @@ __global__ void __launch_bounds__(kPprThreads)
       }
       // the hop itself: hop_advance_rec's draws and choices, written out so
       // the table update above can complete after the column load is issued
-      const Philox4 ph = philox4x32_10((uint32_t)(j + id_shift), hop, sid, 0u, a.seed_lo, a.seed_hi);
-      const uint32_t d0 = ph.x >> 1, d1 = ph.y >> 1;
+      const Draws dr = hop_draws(a, (uint32_t)(j + id_shift), hop, sid, dc);
+      const uint32_t d0 = dr.d0, d1 = dr.d1;
       unsigned long long off = rec >> kDegBits, deg = rec & kDegEscape;
       if (deg == kDegEscape) {
         off = __ldg(g.rowptr + v);
@@ -244,7 +247,7 @@ __global__ void __launch_bounds__(kPprThreads)
         const uint32_t dj = deg > 0 ? d1 : d0;
         if (RULE == GW_RULE_JUMP) {
           next = dj % a.njump;
-          if (ER) next_rec = vertex_rec(g, hp, next);
+          if (ER) next_rec = jump_rec(g, hp, next);
         } else if (RULE == GW_RULE_RESTART || (RULE == GW_RULE_PPR && deg == 0)) {
           next = src;
           next_rec = src_rec;

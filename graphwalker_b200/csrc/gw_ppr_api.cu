@@ -300,6 +300,16 @@ extern "C" gw_status gw_ppr_run(gw_ctx* ctx, const gw_walk_params* params, const
   if (s == GW_OK && !which.empty())
     s = ctx->fail(GW_E_OVERFLOW, "%zu queries still filled their visit tables after %d retries",
                   which.size(), kMaxRetries);
+  if (s != GW_OK) {
+    // The queries without a complete list (still in `which`) get empty rows
+    // (ids all-ones, counts 0), so a partial round-0 list is never mistaken
+    // for a result.  Copies into those rows may still be queued: wait first.
+    cudaStreamSynchronize(st);
+    for (const uint32_t q : which) {
+      std::fill(topk_ids + (size_t)q * k, topk_ids + (size_t)(q + 1) * k, 0xffffffffu);
+      std::fill(topk_counts + (size_t)q * k, topk_counts + (size_t)(q + 1) * k, 0u);
+    }
+  }
   if (stats) *stats = local;
   return s;
 }

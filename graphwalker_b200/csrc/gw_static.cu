@@ -45,67 +45,116 @@ constexpr uint64_t kStaticBytes = align256(kOffBase + kStaticBuckets * 8);
 // cudaGetSymbolAddress (static_scratch_address below).
 static __device__ __align__(256) unsigned char g_superstep_scratch[kStaticBytes];
 
-// Per-device address of g_superstep_scratch, looked up once per device with
-// that device current.
+// Address of g_superstep_scratch in the current device's context.  The
+// lookup runs once per (device, context) with that device current, and again
+// if the device's context changes (after cudaDeviceReset, the primary context
+// is recreated and the array gets a new address).  The driver's context handle
+// comes through the runtime's driver entry point, so the library needs no
+// link to libcuda.  The first lookup on a device must not happen during a
+// stream capture.
 constexpr int kMaxDevices = 64;
+struct ScratchSlot {
+  void* ctx = nullptr;
+  void* addr = nullptr;
+};
 std::mutex g_addr_mutex;
-void* g_addr[kMaxDevices] = {};
+ScratchSlot g_addr[kMaxDevices];
+
+typedef int (*CtxGetCurrentFn)(void**);  // CUresult cuCtxGetCurrent(CUcontext*)
+
+void* current_context() {
+  static CtxGetCurrentFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<CtxGetCurrentFn>(f);
+  }();
+  void* c = nullptr;
+  if (!fn || fn(&c) != 0) return nullptr;
+  return c;
+}
 
 cudaError_t static_scratch_address(int device, unsigned char** out) {
   if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+  // the caller has made `device` current (cudaSetDevice initialises its
+  // primary context), so the driver's current context is that device's
+  void* const cur = current_context();
   std::lock_guard<std::mutex> lock(g_addr_mutex);
-  if (!g_addr[device]) {
+  ScratchSlot& slot = g_addr[device];
+  if (!slot.addr || !cur || slot.ctx != cur) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_superstep_scratch);
     if (e != cudaSuccess) return e;
-    g_addr[device] = p;
+    slot.addr = p;
+    slot.ctx = cur;
   }
-  *out = static_cast<unsigned char*>(g_addr[device]);
+  *out = static_cast<unsigned char*>(slot.addr);
   return cudaSuccess;
 }
 
+// Keeps the calling thread's current device across a call that switches to
+// the context's device.
+struct DeviceGuard {
+  int saved = -1;
+  DeviceGuard() {
+    if (cudaGetDevice(&saved) != cudaSuccess) saved = -1;
+  }
+  ~DeviceGuard() {
+    if (saved >= 0) cudaSetDevice(saved);
+  }
+};
+
 // Exclusive scan of the bucket-major tile histogram in one CTA, then the
 // bucket starts: offsets[d] (first moved walk of destination d), and the
-// per-bucket output pointers the partition scatter writes through.
+// per-bucket output pointers the partition scatter writes through.  Each warp
+// owns one contiguous segment of the histogram and reads it in rows of 32
+// consecutive entries (coalesced): once to total the segment, and once more,
+// after the segment totals are scanned, to write the offsets.
 constexpr int kScanThreads = 1024;
+constexpr int kScanWarps = kScanThreads / 32;
+
+__device__ __forceinline__ uint32_t warp_inclusive_scan(uint32_t x, uint32_t lane) {
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= (uint32_t)d) x += y;
+  }
+  return x;
+}
 
 __global__ void __launch_bounds__(kScanThreads)
     static_scan_kernel(const uint32_t* __restrict__ hist, uint32_t* __restrict__ off, uint32_t m,
                        uint32_t nbuckets, uint32_t ntiles, gw_walk_rec* moved,
                        gw_walk_rec** __restrict__ out_ptr, uint64_t* __restrict__ out_base,
                        uint32_t* __restrict__ offsets) {
-  __shared__ uint32_t warp_sum[kScanThreads / 32];
-  const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const uint32_t chunk = (m + kScanThreads - 1) / kScanThreads;
-  const uint32_t lo = min(m, t * chunk), hi = min(m, lo + chunk);
-  uint32_t sum = 0;
-  for (uint32_t i = lo; i < hi; ++i) sum += hist[i];
-  // inclusive scan of the per-thread sums: inside each warp, then across warps
-  uint32_t x = sum;
+  __shared__ uint32_t seg_base[kScanWarps];
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t seg = ((m + kScanWarps - 1) / kScanWarps + 31) & ~31u;  // whole rows per warp
+  const uint32_t lo = min(m, warp * seg), hi = min(m, lo + seg);
+  uint32_t part = 0;
+  for (uint32_t i = lo + lane; i < hi; i += 32) part += hist[i];
 #pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
-    if (lane >= (uint32_t)d) x += y;
-  }
-  if (lane == 31) warp_sum[warp] = x;
+  for (int d = 16; d > 0; d >>= 1) part += __shfl_xor_sync(0xffffffffu, part, d);
+  if (lane == 0) seg_base[warp] = part;
   __syncthreads();
   if (warp == 0) {
-    uint32_t w = warp_sum[lane];
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, w, d);
-      if (lane >= (uint32_t)d) w += y;
-    }
-    warp_sum[lane] = w;
+    const uint32_t t = seg_base[lane];
+    const uint32_t incl = warp_inclusive_scan(t, lane);
+    seg_base[lane] = incl - t;
   }
   __syncthreads();
-  uint32_t run = x - sum + (warp ? warp_sum[warp - 1] : 0u);  // exclusive prefix of this thread
-  for (uint32_t i = lo; i < hi; ++i) {
-    off[i] = run;
-    run += hist[i];
+  uint32_t carry = seg_base[warp];
+  for (uint32_t row = lo; row < hi; row += 32) {
+    const uint32_t i = row + lane;
+    const uint32_t h = i < hi ? hist[i] : 0u;
+    const uint32_t incl = warp_inclusive_scan(h, lane);
+    if (i < hi) off[i] = carry + incl - h;
+    carry += __shfl_sync(0xffffffffu, incl, 31);
   }
   __syncthreads();
-  for (uint32_t d = t; d < nbuckets; d += kScanThreads) {
+  for (uint32_t d = threadIdx.x; d < nbuckets; d += kScanThreads) {
     const uint32_t start = off[(uint64_t)d * ntiles];
     offsets[d] = start;
     out_ptr[d] = d + 1 < nbuckets ? moved + start : nullptr;
@@ -144,6 +193,7 @@ extern "C" gw_status gw_superstep_static(gw_ctx* ctx, const gw_walk_params* para
   a.hi = ctx->blocks[block + 1];
   cudaStream_t st = (cudaStream_t)stream;  // NULL = the default stream
 
+  DeviceGuard keep_device;  // the caller's current device is restored on return
   GW_CUDA(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
   unsigned char* base = nullptr;
   GW_CUDA(ctx, static_scratch_address(ctx->device, &base), "cudaGetSymbolAddress(scratch)");

@@ -33,6 +33,8 @@ __global__ void __launch_bounds__(kWalkThreads)
   uint32_t st = 0;
   uint32_t clos = 0;
   const L2Hints hp = make_hints(a.hints);
+  DrawCache dc;
+  dc.reset();
   // edge-record mode: the records of the current vertex and of the source
   unsigned long long rec = 0, src_rec = 0;
   if (ER) {
@@ -60,8 +62,8 @@ __global__ void __launch_bounds__(kWalkThreads)
         clos += ((int)hop >= (int)a.L - 1 && v == src) ? 1u : 0u;
       }
       ++k;
-      end = ER ? !hop_advance_carried<RULE>(g, a, hp, id, src, src_rec, hop, v, rec)
-               : !hop_advance<RULE>(g, a, hp, id, src, hop, v);
+      end = ER ? !hop_advance_carried<RULE>(g, a, hp, id, src, src_rec, hop, v, rec, dc)
+               : !hop_advance<RULE>(g, a, hp, id, src, hop, v, dc);
       if (!end) {
         ++hop;
         if (RULE == GW_RULE_RESTART && hop % a.L == a.L - 1) end = true;
@@ -77,6 +79,7 @@ __global__ void __launch_bounds__(kWalkThreads)
       src = w.z;
       hop = w.w;
       k = 0;
+      dc.reset();
       if (ER) {
         rec = vertex_rec(g, hp, v);
         if (rule_returns<RULE>()) src_rec = src == v ? rec : vertex_rec(g, hp, src);
@@ -122,10 +125,12 @@ __global__ void __launch_bounds__(kWalkThreads)
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   uint32_t st = 0, clos = 0;
   const L2Hints hp = make_hints(a.hints);
+  DrawCache dc;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     uint4 w = *(reinterpret_cast<const uint4*>(walks) + i);
     uint32_t v = w.x, id = w.y, src = w.z, hop = w.w;
     bool ended = false;
+    dc.reset();
     while (v >= a.lo && v < a.hi) {
       if (rule_capped<RULE>() && hop >= a.L) break;
       if (RULE == GW_RULE_PROB && hop >= a.max_hops) {
@@ -142,8 +147,8 @@ __global__ void __launch_bounds__(kWalkThreads)
       else if (SINK == GW_SINK_CLOSURE_COUNT)
         clos += ((int)hop >= (int)a.L - 1 && v == src) ? 1u : 0u;
       bool moved;
-      if (SLICE) moved = hop_advance_slice<RULE>(beg_pos, csr, a, id, src, hop, v);
-      else moved = hop_advance<RULE>(g, a, hp, id, src, hop, v);
+      if (SLICE) moved = hop_advance_slice<RULE>(beg_pos, csr, a, id, src, hop, v, dc);
+      else moved = hop_advance<RULE>(g, a, hp, id, src, hop, v, dc);
       if (!moved) {
         ended = true;
         break;

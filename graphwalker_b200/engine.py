@@ -54,16 +54,19 @@ def params(rule: int = RULE_JUMP, sink: int = SINK_VERTEX_COUNT, L: int = 10, *,
            jump_prob: float = 0.15, seed: int = 42, mode: int = MODE_RESIDENT, path_stride: int = 0,
            max_hops: int = 0, prob: float = 0.2, aggregate: bool = False,
            max_supersteps: int = 0, cache_hints: int | None = None, block_lo: int = 0,
-           block_hi: int = 0) -> WalkParams:
+           block_hi: int = 0, rng: int = _lib.RNG_PHILOX) -> WalkParams:
     """gw_walk_params with the reference's defaults (0.15 else-branch, prob 0.2).
     cache_hints: None = engine default, else GW_HINT_* bits used as given.
-    block_lo/block_hi: blocked mode runs only those blocks (block_hi 0 = all)."""
+    block_lo/block_hi: blocked mode runs only those blocks (block_hi 0 = all).
+    rng: RNG_PHILOX (the deterministic mode) or RNG_NATIVE (one Philox block
+    per two hops)."""
     p = WalkParams()
     p.rule, p.sink, p.L, p.njump = rule, sink, L, njump
     p.jump_prob, p.seed, p.mode = jump_prob, seed & 0xFFFFFFFFFFFFFFFF, mode
     p.path_stride, p.max_hops, p.prob, p.aggregate = path_stride, max_hops, prob, int(aggregate)
     p.max_supersteps = max_supersteps
     p.block_lo, p.block_hi = block_lo, block_hi
+    p.rng = rng
     p.cache_hints = 0 if cache_hints is None else (_lib.HINT_EXPLICIT | cache_hints)
     return p
 

@@ -65,6 +65,19 @@ typedef struct gw_ctx gw_ctx;
 #define GW_MODE_RESIDENT 0 /* whole graph in HBM: one launch runs every walk out  */
 #define GW_MODE_BLOCKED 1  /* GraphWalker's block loop: supersteps over one block  */
 
+/* Random stream of the walks.  The reference draws with glibc rand_r seeded
+   per block visit with walkid + dstId + hop + time(NULL)
+   (randomwalkwithjump.hpp:37), a stream no run can reproduce.
+   GW_RNG_PHILOX, the deterministic mode: the two draws of hop h are words 0
+   and 1 of Philox4x32-10(key = seed, counter = (walk id, h, stream, 0)),
+   consumed in the reference's order, so results equal the reference engine's
+   when its rand_r is routed to the same stream.  GW_RNG_NATIVE: one Philox
+   block serves two hops (words 0-1 for hop 2m, words 2-3 for hop 2m+1 of
+   counter (walk id, m, stream, "NATV")); still a function of (seed, walk id,
+   hop), checked statistically against the FP64 power series.             */
+#define GW_RNG_PHILOX 0
+#define GW_RNG_NATIVE 1
+
 #define GW_HINT_EXPLICIT 0x80000000u    /* cache_hints: use exactly these bits     */
 #define GW_HINT_COLUMNS_EVICT_FIRST 1u  /* column loads leave L2 first              */
 #define GW_HINT_COUNTS_EVICT_LAST 2u    /* visit-counter atomics stay in L2         */
@@ -106,7 +119,8 @@ typedef struct gw_walk_params {
                             vertex-partitioned run).  No counterpart in the
                             reference, whose engine runs every block.       */
   uint32_t block_hi;     /* 0 = every block                                 */
-  uint32_t reserved[2];
+  uint32_t rng;          /* GW_RNG_PHILOX (0) or GW_RNG_NATIVE (1)           */
+  uint32_t reserved;
 } gw_walk_params;
 
 typedef struct gw_run_stats {
@@ -224,7 +238,10 @@ typedef struct gw_ppr_stats {
    other queries.  batched = 1: all queries in one persistent walk launch and
    one top-k launch (the replacement of msppr's per-source
    DiscreteDistribution); batched = 0: one query at a time (clear, walk,
-   top-k per query) -- the plain per-query path.  stats may be NULL.      */
+   top-k per query) -- the plain per-query path.  stats may be NULL.
+   On an error return, the rows of queries whose lists are not complete (for
+   GW_E_OVERFLOW, those whose tables still filled after the retries) hold an
+   empty list (ids 0xffffffff, counts 0); the other rows hold their results. */
 gw_status gw_ppr_run(gw_ctx *ctx, const gw_walk_params *params, const uint32_t *sources,
                      const uint32_t *budgets, uint32_t nq, uint32_t k, uint32_t batched,
                      uint32_t *topk_ids, uint32_t *topk_counts, gw_ppr_stats *stats);

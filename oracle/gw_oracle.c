@@ -46,14 +46,24 @@ void gwo_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
 }
 
 /* Per-hop draws: words 0 and 1 of Philox(key=seed, ctr=(id, hop, 0, 0)),
- * each shifted right by one so they span rand_r's [0, RAND_MAX]. */
-static inline void hop_draws(uint64_t seed, uint32_t id, uint32_t hop, uint32_t d[2]) {
+ * each shifted right by one so they span rand_r's [0, RAND_MAX].  The
+ * engine's native-RNG layout (rng = 1) takes both draws of hop h from one
+ * block per two hops: words 0, 1 (h even) or 2, 3 (h odd) of
+ * Philox(ctr = (id, h / 2, 0, "NATV")). */
+#define GWO_NATIVE_TAG 0x4E415456u
+static inline void hop_draws(uint64_t seed, uint32_t rng, uint32_t id, uint32_t hop, uint32_t d[2]) {
     uint32_t ctr[4] = {id, hop, 0u, 0u};
     uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
     uint32_t out[4];
+    int w = 0;
+    if (rng == 1) {
+        ctr[1] = hop >> 1;
+        ctr[3] = GWO_NATIVE_TAG;
+        w = (hop & 1u) ? 2 : 0;
+    }
     gwo_philox4x32_10(ctr, key, out);
-    d[0] = out[0] >> 1;
-    d[1] = out[1] >> 1;
+    d[0] = out[w] >> 1;
+    d[1] = out[w + 1] >> 1;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -111,7 +121,7 @@ uint32_t gwo_get_hop(uint64_t w) { return (uint32_t)(w & 0x3fffu); }
 static inline int hop_advance(const uint64_t *rowptr, const uint32_t *colidx, const gwo_params *p,
                               uint32_t thr, uint32_t id, uint32_t src, uint32_t hop, uint32_t *v) {
     uint32_t d[2];
-    hop_draws(p->seed, id, hop, d);
+    hop_draws(p->seed, p->rng, id, hop, d);
     uint64_t beg = rowptr[*v];
     uint64_t outd = rowptr[*v + 1] - beg;
     int di = 0;

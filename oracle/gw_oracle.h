@@ -74,6 +74,10 @@ typedef struct {
     uint32_t njump;        /* N of `rand_r % N` in the jump rule               */
     uint64_t seed;         /* Philox key                                      */
     uint32_t max_hops;     /* hop guard for the uncapped rule                 */
+    uint32_t rng;          /* 0: draws of hop h = words 0, 1 of Philox(id, h, 0, 0)
+                              (the reference's per-hop draw, shimmed); 1: the
+                              engine's native-RNG layout, words 0-1 (even h) or
+                              2-3 (odd h) of Philox(id, h / 2, 0, "NATV")      */
 } gwo_params;
 
 /*

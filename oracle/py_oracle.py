@@ -27,7 +27,7 @@ ST_BOUNDS, ST_PATH_OVF, ST_HOP_OVF = 1, 2, 4
 
 class Params(Structure):
     _fields_ = [("rule", c_uint32), ("L", c_uint32), ("jump_prob", c_double), ("njump", c_uint32),
-                ("seed", c_uint64), ("max_hops", c_uint32)]
+                ("seed", c_uint64), ("max_hops", c_uint32), ("rng", c_uint32)]
 
 
 def build() -> Path:
@@ -104,12 +104,12 @@ def prob_to_u32(x: float) -> int:
     return min(v, 0xFFFFFFFF)
 
 
-def make_params(rule, L, jump_prob=0.15, njump=0, seed=42, max_hops=65535) -> Params:
-    return Params(rule, L, jump_prob, njump, seed & 0xFFFFFFFFFFFFFFFF, max_hops)
+def make_params(rule, L, jump_prob=0.15, njump=0, seed=42, max_hops=65535, rng=0) -> Params:
+    return Params(rule, L, jump_prob, njump, seed & 0xFFFFFFFFFFFFFFFF, max_hops, rng)
 
 
 def run_walks(rowptr, colidx, cur, *, rule, L, ids=None, src=None, hop0=None, jump_prob=0.15,
-              njump=0, seed=42, max_hops=65535, counts=True, stride=0, closure=False):
+              njump=0, seed=42, max_hops=65535, counts=True, stride=0, closure=False, rng=0):
     """Runs every walk to its end (gw_oracle.h: gwo_run_walks)."""
     rowptr = np.ascontiguousarray(rowptr, dtype=np.uint64)
     colidx = np.ascontiguousarray(colidx, dtype=np.uint32)
@@ -122,7 +122,7 @@ def run_walks(rowptr, colidx, cur, *, rule, L, ids=None, src=None, hop0=None, ju
     ids = src.copy() if ids is None else np.ascontiguousarray(ids, dtype=np.uint32)
     hop0 = np.zeros(n, np.uint32) if hop0 is None else np.ascontiguousarray(
         np.broadcast_to(hop0, (n,)), dtype=np.uint32)
-    prm = make_params(rule, L, jump_prob, njump or nv, seed, max_hops)
+    prm = make_params(rule, L, jump_prob, njump or nv, seed, max_hops, rng)
     out = {}
     c = np.zeros(nv, np.uint32) if counts else None
     paths = np.full(n * stride, 0xFFFFFFFF, np.uint32) if stride else None
@@ -200,7 +200,7 @@ def _chooser_coin(seed: int, superstep: int) -> float:
 
 
 def block_engine(rowptr, colidx, blocks, cur, *, rule, L, ids=None, src=None, hop0=None,
-                 jump_prob=0.15, njump=0, seed=42, prob=0.2, max_hops=65535, max_supersteps=0):
+                 jump_prob=0.15, njump=0, seed=42, prob=0.2, max_hops=65535, max_supersteps=0, rng=0):
     """The reference's block loop (graphwalker.hpp:272-311) over stable pools.
 
     Pools hold walks in arrival order: the walks of a superstep are appended
@@ -225,7 +225,7 @@ def block_engine(rowptr, colidx, blocks, cur, *, rule, L, ids=None, src=None, ho
         m = blk == b
         pools.append([cur[m].copy(), ids[m].copy(), src[m].copy(), hop0[m].copy()])
     minstep = [min(int(p[3].min()), 0xFFFF) if len(p[0]) else 0xFFFF for p in pools]
-    prm = make_params(rule, L, jump_prob, njump or nv, seed, max_hops)
+    prm = make_params(rule, L, jump_prob, njump or nv, seed, max_hops, rng)
     counts = np.zeros(nv, np.uint32)
     status = 0
     superstep = 0

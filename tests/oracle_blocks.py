@@ -35,7 +35,7 @@ class OracleBlocks:
         """Every walk in blocks [p.block_lo, p.block_hi) (all when block_hi is 0)
         advances until it ends or leaves them."""
         lo, hi = (p.block_lo, p.block_hi) if p.block_hi else (0, self.nblocks)
-        prm = self.o.make_params(p.rule, p.L, p.jump_prob, p.njump or self.nv, p.seed, p.max_hops or 65535)
+        prm = self.o.make_params(p.rule, p.L, p.jump_prob, p.njump or self.nv, p.seed, p.max_hops or 65535, p.rng)
         self.counts = np.zeros(self.nv, np.uint32)
         P = self.o._p
         while True:

@@ -35,7 +35,10 @@ def _reference_superstep(gw, G, rule, seed):
     return b, p, G.read_counts(), moved
 
 
-def _static_superstep(gw, G, p, b):
+def _static_superstep(gw, G, p, b, stream=None):
+    """One gw_superstep_static call on `stream` (a torch stream; None = the
+    default stream), then gw_sync on that stream, which also reports the
+    device status word."""
     import torch
     lo, hi = int(G.blocks[b]), int(G.blocks[b + 1])
     v = torch.arange(lo, hi, dtype=torch.int64, device="cuda")
@@ -46,10 +49,12 @@ def _static_superstep(gw, G, p, b):
     offsets = torch.zeros(G.nblocks + 1, dtype=torch.int32, device="cuda")
     minhop = torch.zeros(G.nblocks, dtype=torch.int32, device="cuda")
     lib = gw.load()
+    torch.cuda.synchronize()  # the inputs above were written on torch's stream
+    sh = None if stream is None else stream.cuda_stream
     status = lib.gw_superstep_static(G.handle, ctypes.byref(p), b, walks.data_ptr(), n, counts.data_ptr(),
-                                     moved.data_ptr(), offsets.data_ptr(), minhop.data_ptr(), None)
+                                     moved.data_ptr(), offsets.data_ptr(), minhop.data_ptr(), sh)
     gw._lib.check(status, G.handle)
-    G.sync()
+    G.sync(sh)
     return (counts.cpu().numpy().view(np.uint32), moved.cpu().numpy().view(np.uint32),
             offsets.cpu().numpy().view(np.uint32), minhop.cpu().numpy().view(np.uint32))
 
@@ -80,3 +85,31 @@ def test_superstep_static_rejects_sizes_beyond_its_limit(cuda_device):
         status = lib.gw_superstep_static(G.handle, ctypes.byref(p), 0, 16, (1 << 20) + 1, 16, 16, 16, 16, None)
         assert status == GW_E_INVALID
         assert b"at most" in lib.gw_last_error(G.handle)
+
+
+def test_superstep_static_empty_call_and_side_stream(cuda_device):
+    """An empty call (n = 0, no walk buffers) still writes every output: the
+    offsets all 0 and every block's min hop "no walk" (0xffffffff), whatever
+    the arrays held and whatever the previous call left in the scratch.  A
+    call on a side stream, synchronised through gw_sync on that stream, gives
+    the default-stream call's results."""
+    import torch
+
+    import graphwalker_b200 as gw
+    with gw.Graph.rmat(14, 16, seed=6, blocksize_kb=64) as G:
+        b, p, ref_counts, ref_moved = _reference_superstep(gw, G, gw.RULE_JUMP, 91)
+        default = _static_superstep(gw, G, p, b)  # leaves this superstep in the scratch
+        offsets = torch.full((G.nblocks + 1,), 7, dtype=torch.int32, device="cuda")
+        minhop = torch.full((G.nblocks,), 5, dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        lib = gw.load()
+        gw._lib.check(lib.gw_superstep_static(G.handle, ctypes.byref(p), b, None, 0, None, None,
+                                              offsets.data_ptr(), minhop.data_ptr(), None), G.handle)
+        G.sync()
+        assert np.all(offsets.cpu().numpy() == 0)
+        assert np.all(minhop.cpu().numpy().view(np.uint32) == 0xFFFFFFFF)
+        side = torch.cuda.Stream()
+        got = _static_superstep(gw, G, p, b, stream=side)
+        for x, y in zip(got, default):
+            assert np.array_equal(x, y)
+        assert np.array_equal(got[0], ref_counts)
