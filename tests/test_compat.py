@@ -162,3 +162,61 @@ def test_unchanged_app_preprocesses_a_text_edge_list(cuda_device, tmp_path):
     assert np.array_equal(np.fromfile(d / "graphinfo" / "file_0.csr", np.uint32), gold["rmat10_csr"])
     br = np.array((d / f"blocksize_{kb}KB.blockrange").read_text().split(), np.uint32)
     assert np.array_equal(br, gold["rmat10_blockrange"])
+
+
+def _run_revived(app: str, args: list[str], cwd: Path) -> subprocess.CompletedProcess:
+    exe = APPS_DIR / app
+    if not exe.exists():
+        subprocess.run(["make", "-s", "-C", str(COMPAT), "revived"], check=True)
+    return subprocess.run([str(exe), *args], cwd=cwd, capture_output=True, text=True, timeout=300)
+
+
+@pytest.mark.gpu
+def test_revived_personalizedpagerank_equals_oracle(cuda_device, oracle, tmp_path):
+    """apps/personalizedpagerank.cpp's computation on the live API: R walks
+    from `source` (restart at the source on the 0.15 branch and at dangling
+    vertices, L visits each), counted per vertex.  The 4B.vvalue file it
+    writes equals the oracle's counts for the same walks (walk ids = pool
+    positions, Philox seed 42)."""
+    g = load_golden("rmat13")
+    base = _prepare(tmp_path, g, "rmat13")
+    rp, ci = g["rowptr"], g["colidx"]
+    nv = len(rp) - 1
+    source = int(np.argmax(np.diff(rp.astype(np.int64))))
+    R, L = 3000, 10
+    r = _run_revived("personalizedpagerank", ["file", base, "nvertices", str(nv), "source", str(source), "R", str(R),
+                                              "L", str(L), "shardsize", str(int(g["blocksize_kb"]))], tmp_path)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = np.fromfile(base + "_GraphWalker/4B.vvalue", np.uint32)
+    cur = np.full(R, source, np.uint32)
+    ref = oracle.run_walks(rp, ci, cur, ids=np.arange(R, dtype=np.uint32), src=cur, rule=oracle.RULE_RESTART,
+                           L=L + 1, seed=42)
+    assert np.array_equal(got, ref["counts"])
+    assert int(got.sum()) == R * L
+    # the class accepts only tail = 0, the app's default
+    r = _run_revived("personalizedpagerank", ["file", base, "nvertices", str(nv), "source", str(source), "R", "10",
+                                              "tail", "0.5", "shardsize", str(int(g["blocksize_kb"]))], tmp_path)
+    assert r.returncode != 0
+
+
+@pytest.mark.gpu
+def test_revived_reachability_answers_like_the_oracle(cuda_device, oracle, tmp_path):
+    """apps/reachability.cpp's computation on the live API: whether any of R
+    walks of L visits from a reaches b, for a b the walks reach and a b they
+    do not."""
+    g = load_golden("rmat13")
+    base = _prepare(tmp_path, g, "rmat13")
+    rp, ci = g["rowptr"], g["colidx"]
+    a = int(np.argmax(np.diff(rp.astype(np.int64))))
+    R, L = 200, 12
+    cur = np.full(R, a, np.uint32)
+    ref = oracle.run_walks(rp, ci, cur, ids=np.arange(R, dtype=np.uint32), src=cur, rule=oracle.RULE_RESTART,
+                           L=L + 1, seed=42)["counts"]
+    seen = np.flatnonzero(ref)
+    unseen = np.flatnonzero(ref == 0)
+    cases = {int(seen[np.argmin(ref[seen])]): 1, int(unseen[0]): 0}
+    for b, want in cases.items():
+        r = _run_revived("reachability", ["file", base, "a", str(a), "b", str(b), "R", str(R), "L", str(L),
+                                          "shardsize", str(int(g["blocksize_kb"]))], tmp_path)
+        assert r.returncode == 0, r.stderr[-2000:]
+        assert f"Reachability from {a} to {b} = {want}" in r.stdout

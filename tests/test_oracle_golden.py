@@ -161,3 +161,42 @@ def test_oracle_converter_rejects_what_the_reference_rejects(oracle, text, line)
     asserts, conversions.hpp:226-233); an over-long line would be split by fgets."""
     with pytest.raises(ValueError, match=f"line {line} "):
         oracle.convert_text(text)
+
+
+def _restart_walk_literal(oracle, rp, ci, src, walk_id, nsteps, seed):
+    """RandomWalkwithRestart::updateByWalk (randomwalkwithrestart.hpp:40-51),
+    restated hop by hop in Python: updateInfo, then the test draw (only when
+    the vertex has out-edges), then the neighbour draw; on failure or at a
+    dangling vertex back to the source; nsteps visits."""
+    thr = oracle.continue_threshold(0.15)
+    key = [seed & 0xFFFFFFFF, seed >> 32]
+    v, visits = src, []
+    for hop in range(nsteps):
+        visits.append(v)
+        d = [w >> 1 for w in oracle.philox([walk_id, hop, 0, 0], key)]
+        deg = int(rp[v + 1] - rp[v])
+        if deg > 0 and d[0] >= thr:
+            v = int(ci[int(rp[v]) + d[1] % deg])
+        else:
+            v = src
+    return visits
+
+
+def test_restart_class_is_the_restart_rule_one_segment_longer(oracle):
+    """The revived apps' walk class (RandomWalkwithRestart, nsteps visits from
+    hop 0) runs on the engine as the restart rule with segment length
+    nsteps + 1: per-walk visits equal the literal hop loop's."""
+    g = load_golden("hand")
+    rp, ci = g["rowptr"], g["colidx"]
+    nv = len(rp) - 1
+    seed, nsteps = 0x5EED, 7
+    for src in range(nv):
+        ids = np.arange(40, dtype=np.uint32) + 1000 * src
+        cur = np.full(len(ids), src, np.uint32)
+        r = oracle.run_walks(rp, ci, cur, ids=ids, src=cur, rule=oracle.RULE_RESTART, L=nsteps + 1, seed=seed,
+                             stride=nsteps + 1)
+        assert r["status"] == 0
+        for w, wid in enumerate(ids):
+            want = _restart_walk_literal(oracle, rp, ci, src, int(wid), nsteps, seed)
+            assert int(r["plen"][w]) == nsteps
+            assert r["paths"][w][:nsteps].tolist() == want
