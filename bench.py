@@ -637,10 +637,10 @@ def msppr_measure(args) -> dict:
         # full per-vertex counts come from the same walks (walk j of the batch
         # has Philox id j) run through the resident kernel.
         prefix = np.r_[0, np.cumsum(budgets.astype(np.int64))]
-        acc = []
+        acc, mus = [], {}
         for q in np.argsort(-budgets.astype(np.int64), kind="stable")[:4]:
             src, B = int(sources[q]), int(budgets[q])
-            mu = G.expected_visits(p, src)
+            mu = mus[int(q)] = G.expected_visits(p, src)
             j = torch.arange(prefix[q], prefix[q + 1], dtype=torch.int64, device="cuda")
             w = torch.stack([torch.full_like(j, src), j, torch.full_like(j, src), torch.zeros_like(j)], 1)
             w = w.to(torch.int32).contiguous()
@@ -656,6 +656,17 @@ def msppr_measure(args) -> dict:
             m["query"] = int(q)
             m["batched_list_equals_counts_topk"] = bool(np.array_equal(listed, from_counts))
             acc.append(m)
+        # native-RNG mode: the same batch, judged against the same FP64 series
+        pn = gw.params(gw.RULE_STOP, gw.SINK_NONE, L, seed=args.walk_seed, rng=gw.RNG_NATIVE)
+        G.ppr(pn, sources, budgets, k=args.topk, batched=True)
+        nat_ms = []
+        for _ in range(steps):
+            ids_n, _, stn = G.ppr(pn, sources, budgets, k=args.topk, batched=True)
+            nat_ms.append(stn.ms_total)
+        nat_acc = [{"query": m["query"], **accuracy.measured_accuracy(mus[m["query"]], int(budgets[m["query"]]), L,
+                                                                      ids_n[m["query"]], k=args.topk)} for m in acc]
+        native = {"value": args.queries / (statistics.median(nat_ms) * 1e-3), "unit": "queries/s",
+                  "ms_per_step": statistics.median(nat_ms), "accuracy_vs_fp64": nat_acc}
         cpu = None
         if not args.no_cpu_baseline:
             try:
@@ -684,7 +695,7 @@ def msppr_measure(args) -> dict:
                 "plain": {"value": args.queries / (stp.ms_total * 1e-3), "unit": "queries/s", "ms": stp.ms_total,
                           "launches": stp.launches},
                 "speedup_vs_plain": stp.ms_total / ms_med, "identical_to_plain": same,
-                "accuracy_vs_fp64": acc, "cpu_baseline": cpu,
+                "accuracy_vs_fp64": acc, "native_rng": native, "cpu_baseline": cpu,
                 "e2e": {"value": args.queries / e2e_s, "unit": "queries/s", "ms_per_step": e2e_s * 1e3,
                         "api": "gw_ppr_run (host arrays in, top-k lists out)",
                         "h2d_bytes_per_step": int(args.queries * 8),
@@ -820,6 +831,20 @@ def ppr1_measure(args) -> dict:
         acc = accuracy.measured_accuracy(mu, B, L, ids[0], counts=c, k=100)
         top_from_counts = accuracy.count_topk(np.arange(nv), c, 100)
         acc["top100_api_equals_counts"] = bool(np.array_equal(ids[0][ids[0] != 0xFFFFFFFF], top_from_counts))
+        # native-RNG mode (one Philox block per two hops): timed the same way,
+        # judged against the same FP64 series
+        pn = gw.params(gw.RULE_PPR, gw.SINK_VERTEX_COUNT, L, seed=args.walk_seed, aggregate=True, rng=gw.RNG_NATIVE)
+        for a_, b_ in ev:
+            counts.zero_()
+            a_.record()
+            G.walk_device(pn, walks, B, counts=counts, stream=sh)
+            b_.record()
+        G.sync(sh)
+        ms_native = statistics.median(a_.elapsed_time(b_) for a_, b_ in ev)
+        cn = counts.cpu().numpy().view(np.uint32).copy()
+        native = {"ms_per_step": ms_native, "walk_steps_per_s": int(cn.astype(np.int64).sum()) / (ms_native * 1e-3),
+                  "accuracy_vs_fp64": accuracy.measured_accuracy(mu, B, L, accuracy.count_topk(np.arange(nv), cn, 100),
+                                                                 counts=cn, k=100)}
         return {"metric": "walk-steps/s", "value": nsteps / (ms * 1e-3), "unit": "walk-steps/s", "workload": "ppr1",
                 "n_gpus": 1, "steps": steps, "warmup": max(3, args.warmup), "ms_per_step": ms,
                 "higher_is_better": True, "dtype": "u32", "data": "synthetic",
@@ -830,7 +855,7 @@ def ppr1_measure(args) -> dict:
                 "queries_per_s": 1e3 / ms,
                 "ppr_api": {"device_ms": statistics.median(api_dev), "wall_ms": statistics.median(api_wall),
                             "what": "gw_ppr_run, one query of the same walks, batch tag + walk + top-100, warm"},
-                "accuracy_vs_fp64": acc, "gpu_launches": steps}
+                "accuracy_vs_fp64": acc, "native_rng": native, "gpu_launches": steps}
     finally:
         G.close()
 

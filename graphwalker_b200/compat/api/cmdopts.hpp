@@ -23,6 +23,10 @@
 //   gw_edge_records "auto" (default): 16-byte edge records when they fit in
 //                   half of the free device memory | "on" | "off"
 //                   (gw_set_edge_records)
+//   gw_rng          "philox" (default): the deterministic mode, the draws of
+//                   hop h from Philox(seed; walk id, h) in the reference's
+//                   order | "native": one Philox block per two hops
+//                   (gw_walk_params.rng = GW_RNG_NATIVE)
 #ifndef GRAPHWALKER_CMDOPTS_DEF
 #define GRAPHWALKER_CMDOPTS_DEF
 
