@@ -573,6 +573,19 @@ def e2e_run_pools(args, G, p, rank: int, world: int, K: int, barrier, device_cou
            "api": "gw_run_pools (C ABI, pinned host buffers)"}
     if device_counts is not None:
         out["identical_to_device_step"] = bool(np.array_equal(got, device_counts))
+    # The count read-back cannot overlap the walks: any walk may visit any
+    # vertex up to its last hop, so no count is final before the last walk
+    # ends.  Its cost alone: the same 64 MB device-to-pinned-host copy.
+    dcounts = torch.zeros(nv, dtype=torch.int32, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    d2h = []
+    for _ in range(5):
+        e0.record()
+        hcounts.copy_(dcounts, non_blocking=True)
+        e1.record()
+        e1.synchronize()
+        d2h.append(e0.elapsed_time(e1))
+    out["count_readback_ms"] = statistics.median(d2h)
     return out
 
 
