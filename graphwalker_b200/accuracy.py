@@ -56,14 +56,19 @@ def exact_topk(mu: np.ndarray, k: int) -> np.ndarray:
 def count_topk(ids: np.ndarray, counts: np.ndarray, k: int) -> np.ndarray:
     """Top-k of integer counts over the given ids: count desc, id asc, counts > 0."""
     ids = np.asarray(ids)
-    counts = np.asarray(counts)
+    counts = np.asarray(counts).astype(np.int64)
     keep = counts > 0
     ids, counts = ids[keep], counts[keep]
-    return ids[np.lexsort((ids, -counts.astype(np.int64)))][:k]
+    if len(counts) > 4 * k:
+        # only counts >= the k-th largest can be listed; sort just those
+        kth = np.partition(counts, len(counts) - k)[len(counts) - k]
+        sel = counts >= kth
+        ids, counts = ids[sel], counts[sel]
+    return ids[np.lexsort((ids, -counts))][:k]
 
 
-def expected_accuracy(mu: np.ndarray, budget: int, L: int, k: int = 100, resamples: int = 20,
-                      seed: int = 0, max_candidates: int = 4_000_000) -> dict:
+def expected_accuracy(mu: np.ndarray, budget: int, L: int, k: int = 100, resamples: int = 100,
+                      seed: int = 0, max_candidates: int = 1_000_000) -> dict:
     """The Poisson model's expected L1 error and top-k overlap of a B-walk
     estimate of mu (see the module docstring), with their spreads."""
     mu = np.asarray(mu, dtype=np.float64)
@@ -79,12 +84,14 @@ def expected_accuracy(mu: np.ndarray, budget: int, L: int, k: int = 100, resampl
         out.update(expected_overlap=0.0, overlap_sigma=0.0, candidates=0, resamples=0)
         return out
     # Vertices far below the k-th rate cannot reach the sampled top-k: keep
-    # those whose count could plausibly pass the k-th one (10 sigma each side).
+    # those whose count could plausibly pass the k-th one (7 sigma each side;
+    # a Poisson count beyond 7 sigma has probability below 1e-10).  The
+    # candidates are the highest rates, at most max_candidates of them.
     lam_k = lam[top[-1]]
-    cut = lam_k - 10.0 * np.sqrt(lam_k) - 10.0
+    cut = lam_k - 7.0 * np.sqrt(lam_k) - 7.0
     cand = np.flatnonzero(lam > 0) if cut <= 0 else np.flatnonzero(lam >= _lam_floor(cut))
     if len(cand) > max_candidates:
-        cand = cand[np.argsort(-lam[cand], kind="stable")[:max_candidates]]
+        cand = cand[np.argpartition(-lam[cand], max_candidates - 1)[:max_candidates]]
     rng = np.random.default_rng(seed)
     exact = set(top.tolist())
     ov = []
@@ -98,14 +105,14 @@ def expected_accuracy(mu: np.ndarray, budget: int, L: int, k: int = 100, resampl
 
 
 def _lam_floor(cut: float) -> float:
-    """Smallest rate lam whose count reaches `cut` within 10 sigma:
-    lam + 10 sqrt(lam) + 10 >= cut."""
-    s = max(0.0, -5.0 + np.sqrt(25.0 + max(0.0, cut - 10.0)))
+    """Smallest rate lam whose count reaches `cut` within 7 sigma:
+    lam + 7 sqrt(lam) + 7 >= cut."""
+    s = max(0.0, -3.5 + np.sqrt(12.25 + max(0.0, cut - 7.0)))
     return s * s
 
 
 def measured_accuracy(mu: np.ndarray, budget: int, L: int, top_ids: np.ndarray, counts: np.ndarray | None = None,
-                      k: int = 100, resamples: int = 20, seed: int = 0) -> dict:
+                      k: int = 100, resamples: int = 100, seed: int = 0) -> dict:
     """The measured top-k overlap (and L1 error, when the full per-vertex
     counts are given) beside the model's expectation for the same budget;
     `within_3_sigma` says whether the measurement is no worse than the

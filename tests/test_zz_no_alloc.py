@@ -101,11 +101,13 @@ def test_superstep_static_empty_call_and_side_stream(cuda_device):
         default = _static_superstep(gw, G, p, b)  # leaves this superstep in the scratch
         offsets = torch.full((G.nblocks + 1,), 7, dtype=torch.int32, device="cuda")
         minhop = torch.full((G.nblocks,), 5, dtype=torch.int32, device="cuda")
+        counts = torch.full((G.nv,), 3, dtype=torch.int32, device="cuda")  # the count sink still needs its array
         torch.cuda.synchronize()
         lib = gw.load()
-        gw._lib.check(lib.gw_superstep_static(G.handle, ctypes.byref(p), b, None, 0, None, None,
+        gw._lib.check(lib.gw_superstep_static(G.handle, ctypes.byref(p), b, None, 0, counts.data_ptr(), None,
                                               offsets.data_ptr(), minhop.data_ptr(), None), G.handle)
         G.sync()
+        assert np.all(counts.cpu().numpy() == 3)  # no walk, no visit
         assert np.all(offsets.cpu().numpy() == 0)
         assert np.all(minhop.cpu().numpy().view(np.uint32) == 0xFFFFFFFF)
         side = torch.cuda.Stream()
