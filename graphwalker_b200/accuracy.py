@@ -49,6 +49,10 @@ def exact_topk(mu: np.ndarray, k: int) -> np.ndarray:
     """The k vertices of largest mu, ties broken by the smaller id (only mu > 0)."""
     mu = np.asarray(mu, dtype=np.float64)
     cand = np.flatnonzero(mu > 0)
+    if len(cand) > 4 * k:
+        vals = mu[cand]
+        kth = np.partition(vals, len(vals) - k)[len(vals) - k]
+        cand = cand[vals >= kth]
     order = cand[np.lexsort((cand, -mu[cand]))]
     return order[:k]
 
