@@ -71,10 +71,17 @@ def parse_args():
     ap.add_argument("--no-extras", action="store_true",
                     help="rawwalk at N=1: skip the single-source PPR, msppr and serving sub-objects")
     ap.add_argument("--cpu-sample-sec", type=float, default=15.0)
-    ap.add_argument("--workload", choices=["rawwalk", "msppr", "serve", "ppr1", "ooc", "convert", "simrank"],
+    ap.add_argument("--workload", choices=["rawwalk", "msppr", "serve", "ppr1", "ooc", "convert", "simrank",
+                                           "gather", "walkonly"],
                     default="rawwalk",
                     help="rawwalk: the headline raw-random-walk step; msppr: batched vs plain multi-source PPR; "
-                         "serve: Poisson-arrival PPR serving, continuous batching vs one query per launch")
+                         "serve: Poisson-arrival PPR serving, continuous batching vs one query per launch; "
+                         "gather: the random 32-B sector probe alone (small profiler captures); "
+                         "walkonly: --steps resident walk launches at full occupancy, no autotuner, no extras "
+                         "(small profiler captures)")
+    ap.add_argument("--probe-mb", type=int, default=2048, help="gather: buffer size")
+    ap.add_argument("--probe-loads", type=int, default=1 << 26, help="gather: loads per launch")
+    ap.add_argument("--rng", choices=["philox", "native"], default="philox", help="walkonly: random stream")
     ap.add_argument("--rates", default="1000,5000,10000,20000,50000", help="serve: arrival rates (queries/s)")
     ap.add_argument("--serve-sec", type=float, default=2.0, help="serve: seconds of arrivals per rate")
     ap.add_argument("--nmblocks", type=int, default=0,
@@ -1089,8 +1096,60 @@ def simrank_arm(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def gather_arm(args) -> None:
+    """gw_probe_gather alone: `--probe-loads` loads of 4 B from distinct
+    random 32-B sectors of a `--probe-mb` buffer (a warm-up launch and two
+    timed ones), for profiler captures of the random-miss cost."""
+    import torch
+
+    import graphwalker_b200 as gw
+    torch.cuda.set_device(0)
+    with gw.Graph.rmat(10, 4, seed=1, blocksize_kb=64) as G:
+        buf = torch.zeros(args.probe_mb << 18, dtype=torch.int32, device="cuda")
+        bps = G.probe_gather(buf, buf.numel(), args.probe_loads, iters=2)
+    print(json.dumps({"workload": "gather", "buffer_MB": args.probe_mb, "loads": args.probe_loads,
+                      "useful_GBps_32B": bps / 1e9}), flush=True)
+
+
+def walkonly_arm(args) -> None:
+    """`--steps` launches of the resident walk kernel over one walk per vertex
+    (jump rule, counts), at full occupancy and without the autotuner, for
+    profiler captures at a chosen --scale."""
+    import torch
+
+    import graphwalker_b200 as gw
+    torch.cuda.set_device(0)
+    with gw.Graph.rmat(args.scale, args.edge_factor, seed=args.graph_seed,
+                       blocksize_kb=blocksize_kb_for(args.scale, args.edge_factor, args.nblocks)) as G:
+        layout = "erec" if G.set_edge_records(LAYOUT_MODE[args.layout]) else "csr"
+        nv = G.nv
+        v = torch.arange(nv, dtype=torch.int64, device="cuda")
+        walks = torch.stack([v, v, v, torch.zeros_like(v)], 1).to(torch.int32).contiguous()
+        del v
+        counts = torch.zeros(nv, dtype=torch.int32, device="cuda")
+        p = gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, args.L, seed=args.walk_seed,
+                      rng=gw.RNG_NATIVE if args.rng == "native" else gw.RNG_PHILOX)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(max(1, args.steps))]
+        for a, b in ev:
+            counts.zero_()
+            a.record()
+            G.walk_device(p, walks, nv, counts=counts)
+            b.record()
+        G.sync()
+        visits = int(counts.to(torch.int64).sum().item())
+    print(json.dumps({"workload": "walkonly", "scale": args.scale, "graph_layout": layout, "rng": args.rng,
+                      "launch_ms": [a.elapsed_time(b) for a, b in ev], "visits": visits}), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.workload == "gather" and args.impl != "reference":
+        gather_arm(args)
+        return
+    if args.workload == "walkonly" and args.impl != "reference":
+        walkonly_arm(args)
+        return
     if args.workload == "simrank" and args.impl != "reference":
         simrank_arm(args)
         return

@@ -954,7 +954,9 @@ gw_status gw_walk_autotune(gw_ctx* ctx, const gw_walk_params* params, const gw_w
   cudaEventCreate(&e1);
   int best = max_per_sm;
   float best_ms = 1e30f;
-  for (int c = std::max(1, max_per_sm / 2); c <= max_per_sm; ++c) {
+  // a quarter to full occupancy: a random-miss-bound kernel often runs best
+  // well below full occupancy, where fewer requests queue at the DRAM
+  for (int c = std::max(1, max_per_sm / 4); c <= max_per_sm; ++c) {
     ctx->walk_ctas_per_sm = c;
     float sum = 0.f;
     for (int rep = 0; rep < 4; ++rep) {

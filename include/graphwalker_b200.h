@@ -321,8 +321,8 @@ gw_status gw_pack_words_device(gw_ctx *ctx, const gw_walk_rec *d_walks, uint64_t
 /* Synchronises the stream and returns the device status of earlier kernels. */
 gw_status gw_sync(gw_ctx *ctx, void *stream);
 /* Times the resident walk kernel on the caller's device walks (counts into a
-   scratch array of the context) at each occupancy from half to full CTAs per
-   SM, and keeps the fastest for this context's later resident launches
+   scratch array of the context) at each occupancy from a quarter to full CTAs
+   per SM, and keeps the fastest for this context's later resident launches
    (gw_run, gw_run_pools, gw_walk_device).  The choice changes no result.
    *ctas_per_sm (may be NULL) receives it.  (The reference has no tuner;
    its update loop is an OpenMP loop, graphwalker.hpp:257-270.)            */
