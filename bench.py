@@ -82,6 +82,8 @@ def parse_args():
     ap.add_argument("--probe-mb", type=int, default=2048, help="gather: buffer size")
     ap.add_argument("--probe-loads", type=int, default=1 << 26, help="gather: loads per launch")
     ap.add_argument("--rng", choices=["philox", "native"], default="philox", help="walkonly: random stream")
+    ap.add_argument("--hints", type=int, default=-1,
+                    help="walkonly: explicit GW_HINT_* bits for the walk kernel (-1: the engine default)")
     ap.add_argument("--rates", default="1000,5000,10000,20000,50000", help="serve: arrival rates (queries/s)")
     ap.add_argument("--serve-sec", type=float, default=2.0, help="serve: seconds of arrivals per rate")
     ap.add_argument("--nmblocks", type=int, default=0,
@@ -1128,7 +1130,8 @@ def walkonly_arm(args) -> None:
         del v
         counts = torch.zeros(nv, dtype=torch.int32, device="cuda")
         p = gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, args.L, seed=args.walk_seed,
-                      rng=gw.RNG_NATIVE if args.rng == "native" else gw.RNG_PHILOX)
+                      rng=gw.RNG_NATIVE if args.rng == "native" else gw.RNG_PHILOX,
+                      cache_hints=None if args.hints < 0 else args.hints)
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(max(1, args.steps))]
         for a, b in ev:
@@ -1139,6 +1142,7 @@ def walkonly_arm(args) -> None:
         G.sync()
         visits = int(counts.to(torch.int64).sum().item())
     print(json.dumps({"workload": "walkonly", "scale": args.scale, "graph_layout": layout, "rng": args.rng,
+                      "hints": args.hints,
                       "launch_ms": [a.elapsed_time(b) for a, b in ev], "visits": visits}), flush=True)
 
 

@@ -73,6 +73,7 @@ class PprStats(Structure):
 
 HINT_EXPLICIT = 0x80000000
 HINT_COLUMNS_EVICT_FIRST, HINT_COUNTS_EVICT_LAST, HINT_RECORDS_EVICT_LAST = 1, 2, 4
+HINT_STREAMS_EVICT_FIRST = 8
 
 
 class RunStats(Structure):

@@ -174,7 +174,7 @@ gw_status make_walk_args(gw_ctx* ctx, const gw_walk_params* p, WalkArgs* a) {
     return ctx->fail(GW_E_INVALID, "PATH_RECORD needs path_stride >= 1");
   if (!(p->jump_prob >= 0.0 && p->jump_prob <= 1.0))
     return ctx->fail(GW_E_INVALID, "jump_prob must lie in [0, 1]");
-  a->hints = (p->cache_hints & GW_HINT_EXPLICIT) ? (p->cache_hints & 7u) : kDefaultHints;
+  a->hints = (p->cache_hints & GW_HINT_EXPLICIT) ? (p->cache_hints & 15u) : kDefaultHints;
   a->L = p->L;
   a->thr = gw_continue_threshold(p->jump_prob);
   a->njump = p->njump ? p->njump : ctx->nv;

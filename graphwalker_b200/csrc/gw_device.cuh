@@ -58,6 +58,9 @@ __host__ __device__ __forceinline__ Philox4 philox4x32_10(uint32_t c0, uint32_t 
 constexpr uint32_t kHintColumnsEvictFirst = 1u;
 constexpr uint32_t kHintCountsEvictLast = 2u;
 constexpr uint32_t kHintRecordsEvictLast = 4u;
+// The resident kernel reads every walk record once and every walk's start
+// record once, in order: streams that gain nothing from staying in L2.
+constexpr uint32_t kHintStreamsEvictFirst = 8u;
 
 __device__ __forceinline__ uint64_t l2_policy(bool first, bool last) {
   uint64_t p;
@@ -76,6 +79,14 @@ __device__ __forceinline__ uint32_t ld_nc_u32(const uint32_t* a, uint64_t pol) {
 __device__ __forceinline__ unsigned long long ld_nc_u64(const unsigned long long* a, uint64_t pol) {
   unsigned long long r;
   asm volatile("ld.global.nc.L2::cache_hint.b64 %0, [%1], %2;" : "=l"(r) : "l"(a), "l"(pol));
+  return r;
+}
+
+__device__ __forceinline__ uint4 ld_nc_u32x4(const uint4* a, uint64_t pol) {
+  uint4 r;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+               : "l"(a), "l"(pol));
   return r;
 }
 
@@ -136,7 +147,7 @@ __device__ __forceinline__ constexpr bool rule_capped() {
 // walk ends inside this hop (stop rules); otherwise v is the next vertex and
 // the caller increments the hop.  Loads go through the read-only path.
 struct L2Hints {
-  uint64_t rec, col, cnt, bits;
+  uint64_t rec, col, cnt, bits, strm;
 };
 
 __device__ __forceinline__ L2Hints make_hints(uint32_t flags) {
@@ -145,6 +156,7 @@ __device__ __forceinline__ L2Hints make_hints(uint32_t flags) {
   h.col = l2_policy(flags & kHintColumnsEvictFirst, false);
   h.cnt = l2_policy(false, flags & kHintCountsEvictLast);
   h.bits = l2_policy(false, true);  // the out-edge bitmap is small and read at every jump
+  h.strm = l2_policy(flags & kHintStreamsEvictFirst, false);
   return h;
 }
 

@@ -21,6 +21,21 @@ __device__ __forceinline__ uint4 load_walk(const gw_walk_rec* __restrict__ walks
   return __ldg(reinterpret_cast<const uint4*>(walks) + i);
 }
 
+// The walk record of the resident kernel, read once: with
+// kHintStreamsEvictFirst it is marked to leave L2 first.
+__device__ __forceinline__ uint4 load_walk_hinted(const gw_walk_rec* __restrict__ walks, uint64_t i,
+                                                  const WalkArgs& a, const L2Hints& hp) {
+  return (a.hints & kHintStreamsEvictFirst) ? ld_nc_u32x4(reinterpret_cast<const uint4*>(walks) + i, hp.strm)
+                                            : load_walk(walks, i);
+}
+
+// A walk's start record: like vertex_rec, with the stream policy when asked.
+__device__ __forceinline__ unsigned long long start_rec(const GraphView& g, const WalkArgs& a, const L2Hints& hp,
+                                                        uint32_t v) {
+  if (v >= g.nv) return 0ull;
+  return ld_nc_u64(g.vrec + v, (a.hints & kHintStreamsEvictFirst) ? hp.strm : hp.rec);
+}
+
 template <int RULE, int SINK, bool AGG, bool ER>
 __global__ void __launch_bounds__(kWalkThreads)
     walk_resident_kernel(const gw_walk_rec* __restrict__ walks, uint64_t n, GraphView g,
@@ -28,17 +43,17 @@ __global__ void __launch_bounds__(kWalkThreads)
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  uint4 w = load_walk(walks, i);
+  const L2Hints hp = make_hints(a.hints);
+  uint4 w = load_walk_hinted(walks, i, a, hp);
   uint32_t v = w.x, id = w.y, src = w.z, hop = w.w, k = 0;
   uint32_t st = 0;
   uint32_t clos = 0;
-  const L2Hints hp = make_hints(a.hints);
   DrawCache dc;
   dc.reset();
   // edge-record mode: the records of the current vertex and of the source
   unsigned long long rec = 0, src_rec = 0;
   if (ER) {
-    rec = vertex_rec(g, hp, v);
+    rec = start_rec(g, a, hp, v);
     if (rule_returns<RULE>()) src_rec = src == v ? rec : vertex_rec(g, hp, src);
   }
   for (;;) {
@@ -73,7 +88,7 @@ __global__ void __launch_bounds__(kWalkThreads)
       if (SINK == GW_SINK_PATH_RECORD) s.plen[i] = k;
       i += stride;
       if (i >= n) break;
-      w = load_walk(walks, i);
+      w = load_walk_hinted(walks, i, a, hp);
       v = w.x;
       id = w.y;
       src = w.z;
@@ -81,7 +96,7 @@ __global__ void __launch_bounds__(kWalkThreads)
       k = 0;
       dc.reset();
       if (ER) {
-        rec = vertex_rec(g, hp, v);
+        rec = start_rec(g, a, hp, v);
         if (rule_returns<RULE>()) src_rec = src == v ? rec : vertex_rec(g, hp, src);
       }
     }

@@ -82,6 +82,8 @@ typedef struct gw_ctx gw_ctx;
 #define GW_HINT_COLUMNS_EVICT_FIRST 1u  /* column loads leave L2 first              */
 #define GW_HINT_COUNTS_EVICT_LAST 2u    /* visit-counter atomics stay in L2         */
 #define GW_HINT_RECORDS_EVICT_LAST 4u   /* vertex-record loads stay in L2           */
+#define GW_HINT_STREAMS_EVICT_FIRST 8u  /* walk-record and start-record loads of the
+                                           resident kernel leave L2 first          */
 
 #define GW_RESIDENT_HBM 0  /* CSR copied to device memory once                   */
 #define GW_STREAM_PINNED 1 /* CSR kept in pinned host memory, blocks streamed    */
