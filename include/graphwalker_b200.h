@@ -365,8 +365,10 @@ gw_status gw_simrank_batch(gw_ctx *ctx, const gw_walk_params *params, const uint
    none).  All scratch comes from one fixed device array of the library
    (about 12 MiB per GPU that loads it, held until exit): at most 1,048,576
    walks and 256 blocks per call, else GW_E_INVALID.  The first call on a
-   device looks up that array's address, so make it before any stream
-   capture.  Calls share the array: two calls that overlap on the GPU race. */
+   device (and the first after that device's context was recreated, e.g. by
+   cudaDeviceReset) looks up that array's address, so make it before any
+   stream capture.  The caller's current device is restored on return.
+   Calls share the array: two calls that overlap on the GPU race.          */
 gw_status gw_superstep_static(gw_ctx *ctx, const gw_walk_params *params, uint32_t block,
                               gw_walk_rec *d_walks, uint64_t n, uint32_t *d_counts,
                               gw_walk_rec *d_moved, uint32_t *d_offsets, uint32_t *d_minhop,
