@@ -132,6 +132,24 @@ def test_config1_counts_equal_reference_engine(config1, config1_oracle_counts, o
     assert np.array_equal(np.frombuffer(raw, np.uint32, nv, 8), config1_oracle_counts)
 
 
+def test_config1_streamed_blocks_equal_oracle(config1, config1_oracle_counts):
+    """Config 3's path at config 1's size: the CSR held in pinned host memory,
+    8 device block slots for 33 blocks, the blocked engine (state-aware block
+    choice, block copies on a side stream, eviction of the block with the
+    fewest walks).  Counts equal the oracle's."""
+    import graphwalker_b200 as gw
+    G, _, _ = config1
+    try:
+        G.walks_clear()
+        G.add_walks_at(np.arange(G.nv, dtype=np.uint32))
+        G.set_residency(gw.STREAM_PINNED, nmblocks=8)
+        st = G.run(gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, L1, seed=SEED, mode=gw.MODE_BLOCKED, prob=0.2))
+        assert st.block_loads > 33  # blocks were evicted and loaded again
+        assert np.array_equal(G.read_counts(), config1_oracle_counts)
+    finally:
+        G.set_residency(gw.RESIDENT_HBM)
+
+
 # ---------------------------------------------------------------- config 0
 @pytest.fixture(scope="module")
 def config0(cuda_device, oracle):
