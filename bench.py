@@ -194,10 +194,14 @@ def measured_peaks() -> tuple[float, str]:
 
 def profile_traffic(layout: str) -> float | None:
     """DRAM bytes per walk launch from the committed ncu summary, if any."""
+    return profile_field(layout, "dram_bytes_per_launch")
+
+
+def profile_field(layout: str, key: str) -> float | None:
     f = ROOT / "profiles" / ("walk_resident_rmat24.json" if layout == "csr" else "walk_resident_erec_rmat24.json")
     if f.exists():
         try:
-            return float(json.loads(f.read_text())["dram_bytes_per_launch"])
+            return float(json.loads(f.read_text())[key])
         except Exception:
             return None
     return None
@@ -515,6 +519,15 @@ def our_arm(args) -> None:
     if gather_bps:
         roof["gather_peak_gbs"] = gather_bps / 1e9
         roof["gather_frac"] = achieved / (gather_bps / 1e9)
+        # the line-fill view: a random miss fills a 128-B line, so compare the
+        # kernel's DRAM read rate with the probe's (its useful rate times the
+        # DRAM sectors it reads per 32-B load, from the committed ncu summary)
+        amp = profile_field(layout, "gather_probe_dram_sectors_per_load")
+        if traffic and amp:
+            roof["dram_gbs"] = traffic / (kern_ms * 1e-3) / 1e9
+            roof["probe_dram_gbs"] = gather_bps / 1e9 * amp
+            roof["line_fill_frac"] = roof["dram_gbs"] / roof["probe_dram_gbs"]
+            roof["dram_bytes_per_step"] = traffic / steps_per_launch
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
             "warmup": max(3, args.warmup), "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
