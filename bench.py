@@ -41,11 +41,12 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "walk-steps/s"
 FALLBACK_HBM_GBS = 6650.0
-# Algorithmic DRAM bytes of the headline kernel, per graph layout:
-#   csr:  per step one 32-B sector for the vertex record + one for the column id;
-#   erec: per step one 32-B sector (the edge record moved along, or the vertex
+# Algorithmic DRAM bytes of the headline kernel, per graph layout.  A walk of
+# L visits makes L - 1 moves (the move after its last visit is never observed):
+#   csr:  per move one 32-B sector for the vertex record + one for the column id;
+#   erec: per move one 32-B sector (the edge record moved along, or the vertex
 #         record of a jump target) + one 32-B sector per walk for its start record.
-BYTES_PER_STEP = {"csr": 64, "erec": 32}
+BYTES_PER_MOVE = {"csr": 64, "erec": 32}
 BYTES_PER_WALK = {"csr": 0, "erec": 32}
 LAYOUT_MODE = {"auto": 2, "csr": 0, "erec": 1}  # EDGE_RECORDS_AUTO / _OFF / _ON
 
@@ -507,12 +508,14 @@ def our_arm(args) -> None:
     if rank != 0:
         return
     peak, peak_kind = measured_peaks()
-    algo_bytes = BYTES_PER_STEP[layout] * steps_per_launch + BYTES_PER_WALK[layout] * nv
+    moves = steps_per_launch - nv
+    algo_bytes = BYTES_PER_MOVE[layout] * moves + BYTES_PER_WALK[layout] * nv
     achieved = algo_bytes / (kern_ms * 1e-3) / 1e9
     traffic = profile_traffic(layout)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "peak_source": f"{peak_kind} HBM copy bandwidth",
-            "bytes_per_step": BYTES_PER_STEP[layout], "bytes_per_walk": BYTES_PER_WALK[layout],
+            "bytes_per_move": BYTES_PER_MOVE[layout], "bytes_per_walk": BYTES_PER_WALK[layout],
+            "moves_per_launch": moves,
             "algorithmic_bytes_per_launch": algo_bytes, "graph_layout": layout,
             "kernel": f"walk_resident_kernel<JUMP, VERTEX_COUNT, ER={'true' if layout == 'erec' else 'false'}>",
             "kernel_ms": kern_ms}

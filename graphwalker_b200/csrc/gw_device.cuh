@@ -319,6 +319,20 @@ __device__ __forceinline__ bool hop_advance_carried(const GraphView& g, const Wa
   return false;  // STOP, PROB
 }
 
+// Whether the visit at `hop` is the walk's last: the capped rules visit hops
+// 0 .. L-1, and a restart segment ends on reaching hop % L == L-1.  The move
+// after a last visit is never observed -- the reference's loop tests
+// hop < L (or the segment end) before it uses the vertex it moved to
+// (randomwalkwithjump.hpp:40,55; randomwalkwithrestartwithjoint.hpp:52) --
+// so the kernels skip it, with its draws and its gather.  The uncapped rule
+// has no last visit: its walk ends by the draw itself.
+template <int RULE>
+__device__ __forceinline__ bool last_visit(const WalkArgs& a, uint32_t hop) {
+  if (RULE == GW_RULE_JUMP || RULE == GW_RULE_STOP || RULE == GW_RULE_PPR) return hop + 1 >= a.L;
+  if (RULE == GW_RULE_RESTART) return hop % a.L == (2 * a.L - 2) % a.L;
+  return false;
+}
+
 // Whether a rule's hop can return a walk to its source.
 template <int RULE>
 __device__ __forceinline__ constexpr bool rule_returns() {

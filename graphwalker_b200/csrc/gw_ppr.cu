@@ -200,7 +200,9 @@ __global__ void __launch_bounds__(kPprThreads)
       st |= kStBounds;
       end = true;
     } else {
-      const unsigned long long rec = ER ? cur_rec : ld_nc_u64(g.vrec + v, hp.rec);
+      // the move after a walk's last visit is never observed: skipped
+      const bool last = last_visit<RULE>(a, hop);
+      const unsigned long long rec = (ER || last) ? cur_rec : ld_nc_u64(g.vrec + v, hp.rec);
       ++nvisit;
       // Table update for hops >= 1: lanes visiting the same (query, vertex)
       // fold into one; its first probe (a CAS) is issued now and resolved
@@ -223,36 +225,38 @@ __global__ void __launch_bounds__(kPprThreads)
       }
       // the hop itself: hop_advance_rec's draws and choices, written out so
       // the table update above can complete after the column load is issued
-      const Draws dr = hop_draws(a, (uint32_t)(j + id_shift), hop, sid, dc);
-      const uint32_t d0 = dr.d0, d1 = dr.d1;
-      unsigned long long off = rec >> kDegBits, deg = rec & kDegEscape;
-      if (deg == kDegEscape) {
-        off = __ldg(g.rowptr + v);
-        deg = __ldg(g.rowptr + v + 1) - off;
-      }
       uint32_t next = v;
       unsigned long long next_rec = 0;
-      bool moved = true;
-      if (deg > 0 && d0 >= a.thr) {
-        const unsigned long long r =
-            deg > 0x7fffffffull ? (unsigned long long)d1 : (unsigned long long)(d1 % (uint32_t)deg);
-        if (ER) {
-          const ulonglong2 e = ld_nc_u64x2(g.erec + off + r, hp.col);
-          next = (uint32_t)e.y;
-          next_rec = e.x;
-        } else {
-          next = ld_nc_u32(g.colidx + off + r, hp.col);
+      bool moved = !last;
+      if (!last) {
+        const Draws dr = hop_draws(a, (uint32_t)(j + id_shift), hop, sid, dc);
+        const uint32_t d0 = dr.d0, d1 = dr.d1;
+        unsigned long long off = rec >> kDegBits, deg = rec & kDegEscape;
+        if (deg == kDegEscape) {
+          off = __ldg(g.rowptr + v);
+          deg = __ldg(g.rowptr + v + 1) - off;
         }
-      } else {
-        const uint32_t dj = deg > 0 ? d1 : d0;
-        if (RULE == GW_RULE_JUMP) {
-          next = dj % a.njump;
-          if (ER) next_rec = jump_rec(g, hp, next);
-        } else if (RULE == GW_RULE_RESTART || (RULE == GW_RULE_PPR && deg == 0)) {
-          next = src;
-          next_rec = src_rec;
+        if (deg > 0 && d0 >= a.thr) {
+          const unsigned long long r =
+              deg > 0x7fffffffull ? (unsigned long long)d1 : (unsigned long long)(d1 % (uint32_t)deg);
+          if (ER) {
+            const ulonglong2 e = ld_nc_u64x2(g.erec + off + r, hp.col);
+            next = (uint32_t)e.y;
+            next_rec = e.x;
+          } else {
+            next = ld_nc_u32(g.colidx + off + r, hp.col);
+          }
         } else {
-          moved = false;
+          const uint32_t dj = deg > 0 ? d1 : d0;
+          if (RULE == GW_RULE_JUMP) {
+            next = dj % a.njump;
+            if (ER) next_rec = jump_rec(g, hp, next);
+          } else if (RULE == GW_RULE_RESTART || (RULE == GW_RULE_PPR && deg == 0)) {
+            next = src;
+            next_rec = src_rec;
+          } else {
+            moved = false;
+          }
         }
       }
       if (leader && !table_finish(t, mask, s0, old, qv.tag | v, n, hp.cnt, qv.tag_mask)) qv.full[q] = 1u;

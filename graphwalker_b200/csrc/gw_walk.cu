@@ -77,11 +77,15 @@ __global__ void __launch_bounds__(kWalkThreads)
         clos += ((int)hop >= (int)a.L - 1 && v == src) ? 1u : 0u;
       }
       ++k;
-      end = ER ? !hop_advance_carried<RULE>(g, a, hp, id, src, src_rec, hop, v, rec, dc)
-               : !hop_advance<RULE>(g, a, hp, id, src, hop, v, dc);
-      if (!end) {
-        ++hop;
-        if (RULE == GW_RULE_RESTART && hop % a.L == a.L - 1) end = true;
+      if (last_visit<RULE>(a, hop)) {
+        end = true;  // the move after the last visit is never observed
+      } else {
+        end = ER ? !hop_advance_carried<RULE>(g, a, hp, id, src, src_rec, hop, v, rec, dc)
+                 : !hop_advance<RULE>(g, a, hp, id, src, hop, v, dc);
+        if (!end) {
+          ++hop;
+          if (RULE == GW_RULE_RESTART && hop % a.L == a.L - 1) end = true;
+        }
       }
     }
     if (end) {
@@ -161,6 +165,11 @@ __global__ void __launch_bounds__(kWalkThreads)
       if (SINK == GW_SINK_VERTEX_COUNT) count_visit<AGG>(s.counts, v, hp.cnt);
       else if (SINK == GW_SINK_CLOSURE_COUNT)
         clos += ((int)hop >= (int)a.L - 1 && v == src) ? 1u : 0u;
+      if (last_visit<RULE>(a, hop)) {  // its move is never observed: the walk ends here
+        ++hop;
+        ended = true;
+        break;
+      }
       bool moved;
       if (SLICE) moved = hop_advance_slice<RULE>(beg_pos, csr, a, id, src, hop, v, dc);
       else moved = hop_advance<RULE>(g, a, hp, id, src, hop, v, dc);
