@@ -272,10 +272,24 @@ __device__ __forceinline__ unsigned long long jump_rec(const GraphView& g, const
   return ld_nc_u64(g.vrec + v, hp.rec);
 }
 
+// A jump target with out-edges whose record is not loaded yet.  The load
+// waits for the target's own hop, and happens only if that hop moves along an
+// edge (or never, when the target's visit is the walk's last): its test can
+// fail (a jump needs only "degree > 0", which the bitmap gave), and the last
+// visit makes no move.  No packed record has this value: its offset field
+// would name edge 2^40 - 1.
+constexpr unsigned long long kDeferredRec = ~0ull;
+
+__device__ __forceinline__ unsigned long long jump_rec_deferred(const GraphView& g, const L2Hints& hp, uint32_t v) {
+  if (v >= g.nv) return 0ull;
+  if (g.out_bits) return ((ld_nc_u32(g.out_bits + (v >> 5), hp.bits) >> (v & 31u)) & 1u) ? kDeferredRec : 0ull;
+  return ld_nc_u64(g.vrec + v, hp.rec);
+}
+
 // The same hop over the edge-record layout: the record of v is carried in
 // `rec` from the previous hop.  Moving along an edge reads the next vertex and
-// its record together; a jump reads the record of its target; a return to the
-// source takes the source's record, src_rec, held by the caller.
+// its record together; a jump defers the record of its target (above); a
+// return to the source takes the source's record, src_rec, held by the caller.
 template <int RULE>
 __device__ __forceinline__ bool hop_advance_carried(const GraphView& g, const WalkArgs& a, const L2Hints& hp,
                                                     uint32_t id, uint32_t src, unsigned long long src_rec,
@@ -284,6 +298,16 @@ __device__ __forceinline__ bool hop_advance_carried(const GraphView& g, const Wa
   const Draws dr = hop_draws(a, id, hop, stream, dc);
   const uint32_t d0 = dr.d0;
   const uint32_t d1 = dr.d1;
+  if (rec == kDeferredRec) {
+    // v has out-edges: a failed test jumps with the second draw (outd > 0),
+    // without v's record; a passed one needs it now
+    if (RULE == GW_RULE_JUMP && d0 < a.thr) {
+      v = d1 % a.njump;
+      rec = jump_rec_deferred(g, hp, v);
+      return true;
+    }
+    rec = ld_nc_u64(g.vrec + v, hp.rec);
+  }
   unsigned long long off = rec >> kDegBits;
   unsigned long long deg = rec & kDegEscape;
   if (deg == kDegEscape) {  // mega-hub: exact degree from the row pointer
@@ -302,7 +326,7 @@ __device__ __forceinline__ bool hop_advance_carried(const GraphView& g, const Wa
   const uint32_t dj = deg > 0 ? d1 : d0;
   if (RULE == GW_RULE_JUMP) {
     v = dj % a.njump;
-    rec = jump_rec(g, hp, v);
+    rec = jump_rec_deferred(g, hp, v);
     return true;
   } else if (RULE == GW_RULE_RESTART) {
     v = src;
