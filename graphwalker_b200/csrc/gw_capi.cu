@@ -64,6 +64,7 @@ gw_status init_ctx(gw_ctx* ctx, int device) {
   GW_CUDA(ctx, cudaSetDevice(device), "cudaSetDevice");
   GW_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
   GW_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "stream");
+  GW_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->aux_stream, cudaStreamNonBlocking), "stream");
   GW_CUDA(ctx, ctx->d_status.ensure(sizeof(uint32_t)), "status alloc");
   GW_CUDA(ctx, ctx->h_status.ensure(sizeof(uint32_t)), "status alloc");
   GW_CUDA(ctx, cudaMemsetAsync(ctx->d_status.p, 0, sizeof(uint32_t), ctx->stream), "memset");
@@ -463,6 +464,7 @@ gw_status gw_close(gw_ctx* ctx) {
   if (!ctx) return GW_OK;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+  if (ctx->aux_stream) cudaStreamSynchronize(ctx->aux_stream);
   if (ctx->l2_persist_bytes) gw_set_l2_persisting(ctx, 0);
   for (gw_devbuf* b : {&ctx->d_rowptr, &ctx->d_colidx, &ctx->d_vrec, &ctx->d_erec, &ctx->d_meet, &ctx->d_sr_rows, &ctx->d_blocks,
                        &ctx->d_status,
@@ -480,6 +482,7 @@ gw_status gw_close(gw_ctx* ctx) {
   ctx->h_status.release();
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  if (ctx->aux_stream) cudaStreamDestroy(ctx->aux_stream);
   delete ctx;
   return GW_OK;
 }
@@ -837,12 +840,15 @@ gw_status gw_run_pools(gw_ctx* ctx, const gw_walk_params* params, const uint64_t
   const uint64_t n = pool_offsets[ctx->nblocks];
   if (n && !words) return ctx->fail(GW_E_INVALID, "words is NULL");
   // Chunks of the host words are copied on the copy stream while the walk
-  // kernel of the previous chunk runs on the compute stream.  A walk word
-  // crosses PCIe faster than its walk runs, so the chunks start small (the
-  // first kernel waits only for a short copy) and grow by 7/4 each time,
-  // which keeps each copy shorter than the kernel it hides behind.
+  // kernel of the previous chunk runs.  A walk word crosses PCIe faster than
+  // its walk runs, so the chunks start small (the first kernel waits only for
+  // a short copy) and grow by 7/4 each time, which keeps each copy shorter
+  // than the kernel it hides behind.  The chunk kernels alternate between two
+  // compute streams, so a chunk's walks start while the previous kernel's
+  // last walks finish instead of after them (the walks of different chunks
+  // share only the visit counters, updated atomically).
   std::vector<uint64_t> chunk_lo{0};
-  for (uint64_t m = 1ull << 19; chunk_lo.back() < n; m += m * 3 / 4) chunk_lo.push_back(std::min(n, chunk_lo.back() + m));
+  for (uint64_t m = 1ull << 17; chunk_lo.back() < n; m += m * 3 / 4) chunk_lo.push_back(std::min(n, chunk_lo.back() + m));
   const uint64_t nchunks = chunk_lo.size() - 1;
   GW_CUDA(ctx, ctx->d_walks.ensure(n * sizeof(gw_walk_rec)), "walk alloc");
   GW_CUDA(ctx, ctx->d_words.ensure(n * 8), "word alloc");
@@ -857,10 +863,13 @@ gw_status gw_run_pools(gw_ctx* ctx, const gw_walk_params* params, const uint64_t
   sv.counts = ctx->d_counts.as<uint32_t>();
   std::vector<cudaEvent_t> ready(nchunks);
   for (auto& ev : ready) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
-  cudaEvent_t start_ev;
+  cudaEvent_t start_ev, aux_done;
   cudaEventCreateWithFlags(&start_ev, cudaEventDisableTiming);
-  cudaEventRecord(start_ev, cs);  // copies must not overtake earlier work on cs
+  cudaEventCreateWithFlags(&aux_done, cudaEventDisableTiming);
+  cudaStream_t as = ctx->aux_stream;
+  cudaEventRecord(start_ev, cs);  // copies and kernels must not overtake earlier work on cs
   cudaStreamWaitEvent(xs, start_ev, 0);
+  cudaStreamWaitEvent(as, start_ev, 0);
   cudaError_t e = cudaSuccess;
   for (uint64_t c = 0; c < nchunks && e == cudaSuccess; ++c) {
     const uint64_t lo = chunk_lo[c], m = chunk_lo[c + 1] - lo;
@@ -871,24 +880,29 @@ gw_status gw_run_pools(gw_ctx* ctx, const gw_walk_params* params, const uint64_t
   }
   for (uint64_t c = 0; c < nchunks && e == cudaSuccess; ++c) {
     const uint64_t lo = chunk_lo[c], m = chunk_lo[c + 1] - lo;
-    e = cudaStreamWaitEvent(cs, ready[c], 0);
+    const cudaStream_t ks = (c & 1) ? as : cs;
+    e = cudaStreamWaitEvent(ks, ready[c], 0);
     if (e == cudaSuccess)
       e = gw::launch_unpack_pools(ctx->d_words.as<uint64_t>() + lo,
                                   ids ? ctx->d_ids.as<uint32_t>() + lo : nullptr, lo, m,
                                   ctx->d_pool_offsets.as<uint64_t>(), ctx->d_blocks.as<uint32_t>(),
-                                  ctx->nblocks, ctx->d_walks.as<gw_walk_rec>() + lo, cs);
+                                  ctx->nblocks, ctx->d_walks.as<gw_walk_rec>() + lo, ks);
     cudaAccessPolicyWindow win;
     const bool use_win = params->sink == GW_SINK_VERTEX_COUNT && ctx->counts_window(sv.counts, &win);
     if (e == cudaSuccess)
       e = gw::launch_walk_resident((int)params->rule, (int)params->sink, params->aggregate != 0,
                                    ctx->d_walks.as<gw_walk_rec>() + lo, m, ctx->view(), a, sv,
-                                   ctx->d_status.as<uint32_t>(), gw::resident_grid(ctx, m), cs,
+                                   ctx->d_status.as<uint32_t>(), gw::resident_grid(ctx, m), ks,
                                    use_win ? &win : nullptr);
   }
+  // the counts are complete once both compute streams are done
+  cudaEventRecord(aux_done, as);
+  cudaStreamWaitEvent(cs, aux_done, 0);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(counts, ctx->d_counts.p, (size_t)ctx->nv * 4, cudaMemcpyDeviceToHost, cs);
   for (auto& ev : ready) cudaEventDestroy(ev);
   cudaEventDestroy(start_ev);
+  cudaEventDestroy(aux_done);
   if (e != cudaSuccess) return ctx->cuda_fail(e, "gw_run_pools");
   s = gw::take_status(ctx, cs);
   ctx->last_nwalks = n;

@@ -68,6 +68,7 @@ struct gw_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;       // compute stream
   cudaStream_t copy_stream = nullptr;  // block / walk copies
+  cudaStream_t aux_stream = nullptr;   // second compute stream (gw_run_pools alternates chunk kernels)
   uint32_t residency = GW_RESIDENT_HBM;
   uint32_t nmblocks = 2;
 
