@@ -21,7 +21,16 @@ host program makes (gw_run_pools): 64-bit walk words copied from pinned host
 memory and the counts copied back, every step.  Multi-GPU: the graph is
 replicated, each rank runs its own full walk set (walk ids offset by rank,
 weak scaling) and the visit counts are summed across ranks with one NCCL
-all-reduce per step.
+all-reduce per step, inside the timed step.
+
+At N = 1 the same line also carries, measured in the same run: `parity` (the
+last timed step's counts against the reference engine's own, compiled from
+source with rand_r routed to the same Philox stream), and the other
+workloads as sub-objects -- `ppr1` (single-source PPR, R-MAT scale 20),
+`msppr` (4096 queries at scale 26, batched vs plain, accuracy judged against
+the FP64 series) and `serve` (Poisson arrivals at 1k/10k/50k queries/s,
+continuous batching vs one query per superstep).  --no-extras leaves those
+out.
 """
 from __future__ import annotations
 
