@@ -29,8 +29,9 @@ source with rand_r routed to the same Philox stream), and the other
 workloads as sub-objects -- `ppr1` (single-source PPR, R-MAT scale 20),
 `msppr` (4096 queries at scale 26, batched vs plain, accuracy judged against
 the FP64 series) and `serve` (Poisson arrivals at 1k/10k/50k queries/s,
-continuous batching vs one query per superstep).  --no-extras leaves those
-out.
+continuous batching vs one query per superstep) and `ooc` (R-MAT scale 27,
+edge factor 48, 257 blocks streamed from pinned host memory into 73 % as many
+device slots).  --no-extras leaves those out.
 """
 from __future__ import annotations
 
@@ -552,7 +553,7 @@ def our_arm(args) -> None:
     if world == 1 and not args.no_extras:
         # the other configs' workloads, each measured in this same run
         for key, fn in (("ppr1", ppr1_measure), ("msppr", msppr_measure),
-                        ("serve", lambda a: serve_measure(a, rates="1000,10000,50000"))):
+                        ("serve", lambda a: serve_measure(a, rates="1000,10000,50000")), ("ooc", ooc_measure)):
             t0 = time.perf_counter()
             try:
                 line[key] = fn(args)
@@ -913,55 +914,67 @@ def ppr1_arm(args) -> None:
     print(json.dumps(line), flush=True)
 
 
-def ooc_arm(args) -> None:
+def ooc_measure(args) -> dict:
     """Out-of-core raw random walks: the CSR held in pinned host memory as 256
     blocks, streamed into a bounded number of device block slots by the
     blocked engine (state-aware scheduling, double-buffered copies on a side
-    stream); one walk per vertex, L = 10, 64-bit walk state resident."""
+    stream); one walk per vertex, L = 10, 64-bit walk state resident.  The
+    same walks also run with the graph resident (one launch, and the block
+    loop), and all three give the same counts."""
     import numpy as np
     import torch
 
     import graphwalker_b200 as gw
     torch.cuda.set_device(0)
-    scale = args.scale if args.scale != 24 else 27
+    scale = extra_scale(args, 27)
     ef = args.edge_factor if args.edge_factor != 16 else 48
     nblocks = args.nblocks if args.nblocks != 32 else 256
     kb = blocksize_kb_for(scale, ef, nblocks)
     t0 = time.perf_counter()
     G = gw.Graph.rmat(scale, ef, seed=args.graph_seed, blocksize_kb=kb)
     gen_s = time.perf_counter() - t0
-    nv, L = G.nv, args.L
-    slots = args.nmblocks if args.nmblocks else max(1, (G.nblocks * 73) // 100)
-    graph_bytes = (nv + 1) * 8 + G.ne * 4
-    cur = np.arange(nv, dtype=np.uint32)
-    res = {}
-    # the same walks three ways: one resident launch, the resident block loop, streamed blocks
-    G.walks_clear()
-    G.add_walks_at(cur)
-    del cur
-    for name, residency, mode in (("resident_one_launch", gw.RESIDENT_HBM, gw.MODE_RESIDENT),
-                                  ("resident_blocked", gw.RESIDENT_HBM, gw.MODE_BLOCKED),
-                                  ("streamed_blocked", gw.STREAM_PINNED, gw.MODE_BLOCKED)):
-        G.set_residency(residency, nmblocks=slots)
-        st = G.run(gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, L, seed=args.walk_seed, mode=mode, prob=0.2))
-        total = int(G.read_counts().astype(np.int64).sum())
-        if total != nv * L:
-            raise RuntimeError(f"{name}: {total} visits, expected {nv * L}")
-        res[name] = {"ms": st.ms_total, "walk_steps_per_s": nv * L / (st.ms_total * 1e-3),
-                     "supersteps": int(st.supersteps), "block_loads": int(st.block_loads),
-                     "h2d_GB": st.bytes_h2d / 1e9,
-                     "h2d_GBps": st.bytes_h2d / (st.ms_total * 1e-3) / 1e9 if st.bytes_h2d else 0.0,
-                     "device_ms": {"walk": st.ms_walk, "partition": st.ms_partition, "copy_wait": st.ms_copy_wait}}
-        print(json.dumps({name: res[name]}), flush=True)
-    s = res["streamed_blocked"]
-    line = {"metric": "walk-steps/s", "value": s["walk_steps_per_s"], "unit": "walk-steps/s", "workload": "ooc",
-            "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": s["ms"], "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": f"out-of-core raw random walks, R-MAT scale {scale} ef {ef}, {G.nblocks} blocks in "
-                                   f"pinned host memory, {slots} device block slots, one walk per vertex, "
-                                   f"L={L}, jump rule", "graph_GB": graph_bytes / 1e9, "generate_s": gen_s},
-            "modes": res}
-    G.close()
+    try:
+        nv, L = G.nv, args.L
+        slots = args.nmblocks if args.nmblocks else max(1, (G.nblocks * 73) // 100)
+        graph_bytes = (nv + 1) * 8 + G.ne * 4
+        res, first, same = {}, None, True
+        # the same walks (the context's pools, kept across runs) three ways:
+        # one resident launch, the resident block loop, streamed blocks
+        G.walks_clear()
+        G.add_walks_at(np.arange(nv, dtype=np.uint32))
+        for name, residency, mode in (("resident_one_launch", gw.RESIDENT_HBM, gw.MODE_RESIDENT),
+                                      ("resident_blocked", gw.RESIDENT_HBM, gw.MODE_BLOCKED),
+                                      ("streamed_blocked", gw.STREAM_PINNED, gw.MODE_BLOCKED)):
+            G.set_residency(residency, nmblocks=slots)
+            st = G.run(gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, L, seed=args.walk_seed, mode=mode, prob=0.2))
+            counts = G.read_counts()
+            if int(counts.astype(np.int64).sum()) != nv * L:
+                raise RuntimeError(f"{name}: visit total differs from {nv * L}")
+            if first is None:
+                first = counts
+            else:
+                same = same and bool(np.array_equal(counts, first))
+            res[name] = {"ms": st.ms_total, "walk_steps_per_s": nv * L / (st.ms_total * 1e-3),
+                         "supersteps": int(st.supersteps), "block_loads": int(st.block_loads),
+                         "h2d_GB": st.bytes_h2d / 1e9,
+                         "h2d_GBps": st.bytes_h2d / (st.ms_total * 1e-3) / 1e9 if st.bytes_h2d else 0.0,
+                         "device_ms": {"walk": st.ms_walk, "partition": st.ms_partition,
+                                       "copy_wait": st.ms_copy_wait}}
+        s = res["streamed_blocked"]
+        return {"metric": "walk-steps/s", "value": s["walk_steps_per_s"], "unit": "walk-steps/s", "workload": "ooc",
+                "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": s["ms"], "higher_is_better": True,
+                "dtype": "u32", "data": "synthetic",
+                "config": {"workload": f"out-of-core raw random walks, R-MAT scale {scale} ef {ef}, {G.nblocks} blocks "
+                                       f"in pinned host memory, {slots} device block slots, one walk per vertex, "
+                                       f"L={L}, jump rule", "graph_GB": graph_bytes / 1e9, "generate_s": gen_s},
+                "modes": res, "identical_counts_across_modes": same}
+    finally:
+        G.close()
+
+
+def ooc_arm(args) -> None:
+    line = ooc_measure(args)
+    line["scaling"], line["vs_baseline"] = "weak", None
     print(json.dumps(line), flush=True)
 
 
