@@ -938,14 +938,19 @@ def ooc_measure(args) -> dict:
         slots = args.nmblocks if args.nmblocks else max(1, (G.nblocks * 73) // 100)
         graph_bytes = (nv + 1) * 8 + G.ne * 4
         res, first, same = {}, None, True
-        # the same walks (the context's pools, kept across runs) three ways:
-        # one resident launch, the resident block loop, streamed blocks
+        # the same walks (the context's pools, kept across runs) four ways:
+        # one resident launch, the resident block loop, streamed blocks each
+        # copied into a slot when chosen (findSubGraph), and streamed blocks
+        # with the small pools' blocks read in place (the default)
         G.walks_clear()
         G.add_walks_at(np.arange(nv, dtype=np.uint32))
-        for name, residency, mode in (("resident_one_launch", gw.RESIDENT_HBM, gw.MODE_RESIDENT),
-                                      ("resident_blocked", gw.RESIDENT_HBM, gw.MODE_BLOCKED),
-                                      ("streamed_blocked", gw.STREAM_PINNED, gw.MODE_BLOCKED)):
+        for name, residency, mode, mapped in (
+                ("resident_one_launch", gw.RESIDENT_HBM, gw.MODE_RESIDENT, gw.MAPPED_AUTO),
+                ("resident_blocked", gw.RESIDENT_HBM, gw.MODE_BLOCKED, gw.MAPPED_AUTO),
+                ("streamed_blocked_copy_all", gw.STREAM_PINNED, gw.MODE_BLOCKED, 0),
+                ("streamed_blocked", gw.STREAM_PINNED, gw.MODE_BLOCKED, gw.MAPPED_AUTO)):
             G.set_residency(residency, nmblocks=slots)
+            G.set_mapped_block_walks(mapped)
             st = G.run(gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, L, seed=args.walk_seed, mode=mode, prob=0.2))
             counts = G.read_counts()
             if int(counts.astype(np.int64).sum()) != nv * L:
@@ -958,8 +963,13 @@ def ooc_measure(args) -> dict:
                          "supersteps": int(st.supersteps), "block_loads": int(st.block_loads),
                          "h2d_GB": st.bytes_h2d / 1e9,
                          "h2d_GBps": st.bytes_h2d / (st.ms_total * 1e-3) / 1e9 if st.bytes_h2d else 0.0,
+                         "blocks_read_in_place": {"supersteps": int(st.mapped_supersteps),
+                                                  "walks": int(st.mapped_walks)},
                          "device_ms": {"walk": st.ms_walk, "partition": st.ms_partition,
                                        "copy_wait": st.ms_copy_wait}}
+        link = host_link_gbps()
+        for r in res.values():
+            r["h2d_link_utilisation"] = r["h2d_GBps"] / link
         s = res["streamed_blocked"]
         return {"metric": "walk-steps/s", "value": s["walk_steps_per_s"], "unit": "walk-steps/s", "workload": "ooc",
                 "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": s["ms"], "higher_is_better": True,
@@ -967,9 +977,29 @@ def ooc_measure(args) -> dict:
                 "config": {"workload": f"out-of-core raw random walks, R-MAT scale {scale} ef {ef}, {G.nblocks} blocks "
                                        f"in pinned host memory, {slots} device block slots, one walk per vertex, "
                                        f"L={L}, jump rule", "graph_GB": graph_bytes / 1e9, "generate_s": gen_s},
-                "modes": res, "identical_counts_across_modes": same}
+                "host_link_GBps": link, "modes": res, "identical_counts_across_modes": same,
+                "speedup_vs_copy_all": res["streamed_blocked_copy_all"]["ms"] / s["ms"]}
     finally:
         G.close()
+
+
+def host_link_gbps() -> float:
+    """Host-to-device rate of one 1 GiB copy from pinned memory (best of 3),
+    the denominator of the streamed runs' link utilisation."""
+    import torch
+    src = torch.empty(1 << 30, dtype=torch.uint8).pin_memory()
+    dst = torch.empty(1 << 30, dtype=torch.uint8, device="cuda")
+    best = 0.0
+    for _ in range(3):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        dst.copy_(src, non_blocking=True)
+        b.record()
+        torch.cuda.synchronize()
+        best = max(best, (1 << 30) / (a.elapsed_time(b) * 1e-3) / 1e9)
+    del src, dst
+    torch.cuda.empty_cache()
+    return best
 
 
 def ooc_arm(args) -> None:

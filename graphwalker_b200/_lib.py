@@ -23,6 +23,7 @@ SINK_NONE, SINK_VERTEX_COUNT, SINK_PATH_RECORD, SINK_CLOSURE_COUNT = 0, 1, 2, 3
 MODE_RESIDENT, MODE_BLOCKED = 0, 1
 RNG_PHILOX, RNG_NATIVE = 0, 1
 RESIDENT_HBM, STREAM_PINNED = 0, 1
+MAPPED_AUTO = (1 << 64) - 1  # gw_set_mapped_block_walks: per block, one walk per 128 CSR bytes
 
 
 class WalkRec(Structure):
@@ -79,7 +80,8 @@ HINT_STREAMS_EVICT_FIRST = 8
 class RunStats(Structure):
     _fields_ = [("walks", c_uint64), ("supersteps", c_uint64), ("block_loads", c_uint64),
                 ("bytes_h2d", c_uint64), ("ms_total", c_double), ("ms_walk", c_double),
-                ("ms_partition", c_double), ("ms_copy_wait", c_double)]
+                ("ms_partition", c_double), ("ms_copy_wait", c_double), ("mapped_supersteps", c_uint64),
+                ("mapped_walks", c_uint64)]
 
 
 class GraphDesc(Structure):
@@ -115,6 +117,7 @@ _SIGS = {
     "gw_get_blocks": (c_int32, [_P, _P, c_uint32]),
     "gw_export_csr": (c_int32, [_P, _P, _P]),
     "gw_set_residency": (c_int32, [_P, c_uint32, c_uint32]),
+    "gw_set_mapped_block_walks": (c_int32, [_P, c_uint64]),
     "gw_walks_clear": (c_int32, [_P]),
     "gw_walks_add": (c_int32, [_P, c_uint32, _P, _P, c_size_t]),
     "gw_walks_count": (c_int32, [_P, _P, POINTER(c_uint64)]),

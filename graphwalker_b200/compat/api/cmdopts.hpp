@@ -18,6 +18,11 @@
 //                   the counts to RandomWalk::gw_deliver_counts
 //   gw_mode         "resident" (default) | "blocked"
 //   gw_residency    "hbm" (default) | "stream"
+//   gw_mapped_walks streamed blocks with at most this many pending walks are
+//                   read in place from pinned host memory, not copied:
+//                   "auto" (default, per block one walk per 128 bytes of its
+//                   CSR) | a number | 0 (copy every block)
+//                   (gw_set_mapped_block_walks)
 //   gw_chunk        walks per device run in replay mode (default 4194304)
 //   gw_device       CUDA device ordinal (default 0)
 //   gw_edge_records "auto" (default): 16-byte edge records when they fit in

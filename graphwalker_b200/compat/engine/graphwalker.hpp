@@ -18,6 +18,7 @@
 #include <omp.h>
 #include <sys/time.h>
 
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -60,6 +61,10 @@ class graphwalker_engine {
     if (gw_open(&d, &ctx) != GW_OK)
       logstream(LOG_FATAL) << "graphwalker_engine: " << gw_last_error(nullptr) << std::endl;
     m.stop_time("2_findSubGraph");
+    const std::string mapped = get_option_string("gw_mapped_walks", "auto");
+    if (gw_set_mapped_block_walks(ctx, mapped == "auto" ? GW_MAPPED_AUTO : strtoull(mapped.c_str(), nullptr, 10)) !=
+        GW_OK)
+      logstream(LOG_FATAL) << "graphwalker_engine: " << gw_last_error(ctx) << std::endl;
     const std::string erec = get_option_string("gw_edge_records", "auto");
     uint32_t erec_built = 0;
     if (gw_set_edge_records(ctx, erec == "on" ? GW_EDGE_RECORDS_ON : erec == "off" ? GW_EDGE_RECORDS_OFF
@@ -185,6 +190,7 @@ class graphwalker_engine {
     m.add("gpu_ms_walk", st.ms_walk);
     m.add("gpu_ms_partition", st.ms_partition);
     m.add("gpu_ms_copy_wait", st.ms_copy_wait);
+    m.add("gpu_blocks_read_in_place", (double)st.mapped_supersteps, INTEGER);
   }
 
   // Runs the walks in chunks that record paths on the device, then calls

@@ -550,6 +550,12 @@ gw_status gw_set_residency(gw_ctx* ctx, uint32_t residency, uint32_t nmblocks) {
   return apply_edge_records(ctx);
 }
 
+gw_status gw_set_mapped_block_walks(gw_ctx* ctx, uint64_t max_walks) {
+  if (!ctx) return set_thread_error(GW_E_INVALID, "NULL context");
+  ctx->mapped_max_walks = max_walks;
+  return GW_OK;
+}
+
 gw_status gw_simrank_meet(gw_ctx* ctx, const uint32_t* d_paths_a, const uint32_t* d_paths_b, uint32_t R,
                           uint32_t L, uint64_t* meet, void* stream) {
   if (!ctx) return set_thread_error(GW_E_INVALID, "NULL context");

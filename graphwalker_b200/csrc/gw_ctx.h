@@ -71,6 +71,7 @@ struct gw_ctx {
   cudaStream_t aux_stream = nullptr;   // second compute stream (gw_run_pools alternates chunk kernels)
   uint32_t residency = GW_RESIDENT_HBM;
   uint32_t nmblocks = 2;
+  uint64_t mapped_max_walks = GW_MAPPED_AUTO;  // streamed blocks read in place at or below this many walks
 
   // graph
   uint32_t nv = 0;

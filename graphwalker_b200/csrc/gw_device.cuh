@@ -370,10 +370,10 @@ __device__ __forceinline__ constexpr bool rule_returns() {
 template <int RULE>
 __device__ __forceinline__ bool hop_advance_slice(const unsigned long long* __restrict__ beg_pos,
                                                   const uint32_t* __restrict__ csr,
-                                                  const WalkArgs& a, uint32_t id, uint32_t src,
-                                                  uint32_t hop, uint32_t& v, DrawCache& dc) {
+                                                  unsigned long long b0, const WalkArgs& a,
+                                                  uint32_t id, uint32_t src, uint32_t hop,
+                                                  uint32_t& v, DrawCache& dc) {
   const uint32_t vl = v - a.lo;
-  const unsigned long long b0 = __ldg(beg_pos);
   const unsigned long long b = __ldg(beg_pos + vl);
   const unsigned long long deg = __ldg(beg_pos + vl + 1) - b;
   const Draws dr = hop_draws(a, id, hop, 0u, dc);

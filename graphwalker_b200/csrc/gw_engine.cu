@@ -9,12 +9,22 @@
 // Each superstep picks a block with the reference's state-aware policy (with
 // probability `prob` the block holding the lowest-hop walk, otherwise the
 // block with the most pending walks), makes its CSR available (resident HBM,
-// or a slot filled from pinned host memory by async copies on a side stream,
-// prefetching the next likely block while the current one runs), advances
-// every walk of its pool while it stays inside the block, and stably
+// or a slot filled from pinned host memory by async copies on a side stream),
+// advances every walk of its pool while it stays inside the block, and stably
 // partitions the walks that left into the pools of their new blocks.  The
 // per-block pending counts and minimum hops the policy reads come back from
-// the partition's histogram each superstep.
+// the partition's histogram each superstep, through mapped pinned memory, so
+// no small copy of a superstep queues behind a block copy.
+//
+// Streaming differs from findSubGraph in two ways that change neither the
+// order of blocks nor any walk:
+//  * a chosen block in no slot whose pool is small (ctx->mapped_max_walks,
+//    or per block its CSR bytes / kMappedBytesPerWalk) is read in place from
+//    the pinned host copy through its mapped device address: its walks fetch
+//    a few sectors per hop over the host link instead of the whole block;
+//  * while a block runs, up to kCopyAhead blocks with many pending walks are
+//    copied into slots before their turn, each taking the room of the slot
+//    with the fewest pending walks (swapOut's victim) when it has more.
 #include <algorithm>
 #include <cstring>
 
@@ -25,6 +35,14 @@ namespace gw {
 namespace {
 
 constexpr uint32_t kNoBlock = 0xffffffffu;
+// GW_MAPPED_AUTO: a streamed block runs in place when it has at most one
+// pending walk per this many bytes of its CSR.  Copying a block costs its
+// bytes at the host link's rate; a walk run in place costs a few sectors
+// fetched over the same link and waits on their latency.
+constexpr uint64_t kMappedBytesPerWalk = 128;
+// Blocks copied ahead of their turn at most (1 to 5 measured within 2 % of
+// one another on an out-of-core scale-27 graph, the deeper the faster).
+constexpr size_t kCopyAhead = 3;
 
 struct Slots {
   // One device slot holds the CSR slice of one block:
@@ -143,7 +161,9 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
 
   // ---- partition scratch ----
   const uint32_t nbk = nb + 1;  // + the "ended" bucket
-  GW_CUDA(ctx, ctx->d_totals.ensure(2 * nbk * 4), "totals alloc");  // totals | minhop
+  GW_CUDA(ctx, ctx->d_totals.ensure(nbk * 4), "minhop alloc");  // per-bucket minimum hop
+  // cleared once; each superstep's totals kernel resets it after reading it
+  GW_CUDA(ctx, cudaMemsetAsync(ctx->d_totals.p, 0xff, nbk * 4, st), "minhop clear");
   GW_CUDA(ctx, ctx->d_out_ptr.ensure(nbk * sizeof(void*)), "ptr alloc");
   GW_CUDA(ctx, ctx->d_out_base.ensure(nbk * 8), "base alloc");
   gw_hostbuf h_xfer;  // pinned: totals|minhop down, ptr|base up
@@ -152,6 +172,14 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
   uint32_t* h_minhop = h_totals + nbk;
   gw_walk_rec** h_ptr = reinterpret_cast<gw_walk_rec**>(h_totals + 2 * nbk);
   uint64_t* h_base = reinterpret_cast<uint64_t*>(h_ptr + nbk);
+  // The device reaches h_xfer at its mapped address: the totals kernel writes
+  // totals|minhop there and a fetch kernel reads ptr|base, so the small
+  // transfers of a superstep never wait behind a block copy on the copy engine.
+  void* m_xfer = nullptr;
+  GW_CUDA(ctx, cudaHostGetDevicePointer(&m_xfer, h_xfer.p, 0), "mapped scratch");
+  uint32_t* m_totals = static_cast<uint32_t*>(m_xfer);
+  const uint64_t* m_ptr = reinterpret_cast<const uint64_t*>(m_totals + 2 * nbk);
+  const uint64_t* m_base = m_ptr + nbk;
 
   // ---- streamed block slots ----
   Slots slots;
@@ -177,9 +205,29 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
       cudaEventRecord(slots.free_ev[i], st);
     }
   }
+  // mapped device addresses of the pinned host CSR (blocks read in place)
+  const unsigned long long* m_rowptr = nullptr;
+  const uint32_t* m_colidx = nullptr;
+  if (streaming && ctx->mapped_max_walks) {
+    void* mp = nullptr;
+    GW_CUDA(ctx, cudaHostGetDevicePointer(&mp, ctx->h_rowptr.p, 0), "mapped rowptr");
+    m_rowptr = static_cast<const unsigned long long*>(mp);
+    GW_CUDA(ctx, cudaHostGetDevicePointer(&mp, ctx->h_colidx.p, 0), "mapped colidx");
+    m_colidx = static_cast<const uint32_t*>(mp);
+  }
+  // the most pending walks at which block q runs in place (0 = never)
+  auto mapped_limit = [&](uint32_t q) -> uint64_t {
+    if (!m_rowptr) return 0;
+    if (ctx->mapped_max_walks != GW_MAPPED_AUTO) return ctx->mapped_max_walks;
+    const uint64_t* hr = ctx->h_rowptr.as<uint64_t>();
+    const uint64_t bytes = ((uint64_t)ctx->blocks[q + 1] - ctx->blocks[q] + 1) * 8 +
+                           (hr[ctx->blocks[q + 1]] - hr[ctx->blocks[q]]) * 4;
+    return bytes / kMappedBytesPerWalk;
+  };
   ctx->stats = gw_run_stats{};
   ctx->stats.walks = nwalks;
 
+  std::vector<uint32_t> ahead;  // blocks copied ahead of their turn, not yet run
   // findSubGraph: make block b resident in a slot (never the slot `keep`).
   auto load_block = [&](uint32_t b, int keep) -> int {
     if (slots.slot_of[b] >= 0) return slots.slot_of[b];
@@ -197,6 +245,7 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
         }
       }
       slots.slot_of[slots.block[victim]] = -1;
+      ahead.erase(std::remove(ahead.begin(), ahead.end(), slots.block[victim]), ahead.end());
     }
     const uint64_t* hr = ctx->h_rowptr.as<uint64_t>();
     const uint32_t v0 = ctx->blocks[b], v1 = ctx->blocks[b + 1];
@@ -292,10 +341,19 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     cudaEvent_t* ph = phase_set(superstep);
     cudaEventRecord(ph[0], st);
     if (streaming) {
-      slot = load_block(b, -1);
-      cudaStreamWaitEvent(st, slots.ready[slot], 0);
-      beg_pos = slots.beg_pos[slot].as<unsigned long long>();
-      csr = slots.csr[slot].as<uint32_t>();
+      ahead.erase(std::remove(ahead.begin(), ahead.end(), b), ahead.end());
+      if (slots.slot_of[b] < 0 && n <= mapped_limit(b)) {
+        const uint64_t e0 = ctx->h_rowptr.as<uint64_t>()[ab.lo];
+        beg_pos = m_rowptr + ab.lo;
+        csr = m_colidx + e0;
+        ctx->stats.mapped_supersteps++;
+        ctx->stats.mapped_walks += n;
+      } else {
+        slot = load_block(b, -1);
+        cudaStreamWaitEvent(st, slots.ready[slot], 0);
+        beg_pos = slots.beg_pos[slot].as<unsigned long long>();
+        csr = slots.csr[slot].as<uint32_t>();
+      }
     }
     // ---- exec_updates ----
     cudaEventRecord(ph[1], st);
@@ -305,28 +363,40 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     if (e != cudaSuccess) break;
     cudaEventRecord(ph[2], st);
     if (streaming) {
-      cudaEventRecord(slots.free_ev[slot], st);
-      // prefetch the block most likely chosen next while this one runs
-      uint64_t best = 0;
-      uint32_t nxt = kNoBlock;
-      for (uint32_t q = 0; q < nb; ++q)
-        if (q != b && ctx->pool_size[q] > best) {
-          best = ctx->pool_size[q];
-          nxt = q;
+      if (slot >= 0) cudaEventRecord(slots.free_ev[slot], st);
+      // Copy ahead: keep up to kCopyAhead blocks copied before their turn,
+      // so the host link stays busy while blocks in slots run.  The candidate
+      // is the block in no slot with the most pending walks (more than it
+      // needs to be read in place); it takes the room of the slot with the
+      // fewest pending walks, and only when it has more.
+      while (ahead.size() < kCopyAhead) {
+        uint64_t best = 0;
+        uint32_t nxt = kNoBlock;
+        for (uint32_t q = 0; q < nb; ++q)
+          if (q != b && slots.slot_of[q] < 0 && ctx->pool_size[q] > best && ctx->pool_size[q] > mapped_limit(q)) {
+            best = ctx->pool_size[q];
+            nxt = q;
+          }
+        if (nxt == kNoBlock) break;
+        bool room = false;
+        uint64_t minw = ~0ull;
+        for (uint32_t i = 0; i < nslots; ++i) {
+          if ((int)i == slot) continue;
+          if (slots.block[i] == kNoBlock) room = true;
+          else minw = std::min<uint64_t>(minw, ctx->pool_size[slots.block[i]]);
         }
-      if (nxt != kNoBlock && slots.slot_of[nxt] < 0 && nslots > 1) load_block(nxt, slot);
+        if (!room && best <= minw) break;
+        load_block(nxt, slot);
+        ahead.push_back(nxt);
+      }
     }
     // ---- moveWalk: stable partition by destination block ----
-    uint32_t* d_tot = ctx->d_totals.as<uint32_t>();
-    uint32_t* d_minhop = d_tot + nbk;
-    GW_CUDA(ctx, cudaMemsetAsync(d_minhop, 0xff, nbk * 4, st), "minhop clear");
+    uint32_t* d_minhop = ctx->d_totals.as<uint32_t>();
     e = launch_partition_hist(ctx->pools[b].as<gw_walk_rec>(), ctx->d_dest.as<uint32_t>(), n, plan,
                               ctx->d_tile_hist.as<uint32_t>(), d_minhop, st);
     if (e == cudaSuccess)
-      e = launch_partition_scan(ctx->d_tile_hist.as<uint32_t>(), ctx->d_tile_off.as<uint32_t>(), d_tot,
-                                plan, ctx->d_scan_temp.p, st);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(h_totals, d_tot, 2 * nbk * 4, cudaMemcpyDeviceToHost, st);
+      e = launch_partition_scan(ctx->d_tile_hist.as<uint32_t>(), ctx->d_tile_off.as<uint32_t>(), m_totals,
+                                plan, ctx->d_scan_temp.p, st, d_minhop, m_totals + nbk);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) break;
     if (superstep > 0) add_phases(superstep - 1);
@@ -360,9 +430,8 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     if (e != cudaSuccess) break;
     h_ptr[nb] = nullptr;
     h_base[nb] = 0;
-    e = cudaMemcpyAsync(ctx->d_out_ptr.p, h_ptr, nbk * sizeof(void*), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(ctx->d_out_base.p, h_base, nbk * 8, cudaMemcpyHostToDevice, st);
+    e = launch_fetch_u64_pair(m_ptr, ctx->d_out_ptr.as<uint64_t>(), m_base, ctx->d_out_base.as<uint64_t>(),
+                              nbk, st);
     if (e == cudaSuccess)
       e = launch_partition_scatter(ctx->pools[b].as<gw_walk_rec>(), ctx->d_dest.as<uint32_t>(), n, plan,
                                    ctx->d_tile_off.as<uint32_t>(),
@@ -370,8 +439,8 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
                                    ctx->d_out_base.as<uint64_t>(), st);
     if (e != cudaSuccess) break;
     cudaEventRecord(ph[3], st);
-    // h_ptr/h_base are rewritten only after the next totals wait, when these
-    // up-copies have landed
+    // h_ptr/h_base are rewritten only after the next totals wait, when the
+    // fetch kernel has read them
     pending = true;
     uint64_t forwarded = 0;
     for (uint32_t d = 0; d < nb; ++d) {

@@ -95,9 +95,19 @@ cudaError_t launch_partition_hist(const gw_walk_rec* walks, const uint32_t* dest
                                   const PartitionPlan& plan, uint32_t* tile_hist,
                                   uint32_t* minhop, cudaStream_t stream);
 // Exclusive scan of tile_hist (bucket-major) into tile_off, and per-bucket
-// totals.
+// totals; with minhop_src, also moves the nbuckets minimum hops to
+// minhop_dst and resets minhop_src to 0xffffffff for the next histogram
+// (totals and minhop_dst may be mapped pinned host memory, which the host
+// reads after a stream synchronisation, with no copy call).
 cudaError_t launch_partition_scan(const uint32_t* tile_hist, uint32_t* tile_off, uint32_t* totals,
-                                  const PartitionPlan& plan, void* temp, cudaStream_t stream);
+                                  const PartitionPlan& plan, void* temp, cudaStream_t stream,
+                                  uint32_t* minhop_src = nullptr, uint32_t* minhop_dst = nullptr);
+// dst_a[i] = src_a[i], dst_b[i] = src_b[i] for i < n, by a kernel: the
+// sources may be mapped pinned host memory written by the host before the
+// launch.  Unlike an async host-to-device copy this does not queue behind
+// large block copies on the copy engine.
+cudaError_t launch_fetch_u64_pair(const uint64_t* src_a, uint64_t* dst_a, const uint64_t* src_b,
+                                  uint64_t* dst_b, uint32_t n, cudaStream_t stream);
 // Stable scatter: walk i with dest d lands at out_ptr[d][out_base[d] + rank],
 // rank = position among the walks with dest d in input order.  Bucket
 // nbuckets-1 (ended walks) is not written.

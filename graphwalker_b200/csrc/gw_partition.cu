@@ -11,6 +11,8 @@
 // lanes; stability inside a tile comes from a warp match on the destination
 // and the rank among lower lanes, across tiles from an exclusive scan over a
 // bucket-major histogram.
+#include <algorithm>
+
 #include <cub/device/device_scan.cuh>
 
 #include "gw_internal.h"
@@ -53,11 +55,25 @@ __global__ void __launch_bounds__(kPartThreads)
 
 __global__ void partition_totals_kernel(const uint32_t* __restrict__ tile_hist,
                                         const uint32_t* __restrict__ tile_off, uint32_t nbuckets,
-                                        uint32_t ntiles, uint32_t* __restrict__ totals) {
+                                        uint32_t ntiles, uint32_t* __restrict__ totals,
+                                        uint32_t* __restrict__ minhop_src,
+                                        uint32_t* __restrict__ minhop_dst) {
   for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nbuckets;
        b += gridDim.x * blockDim.x) {
     const uint64_t first = (uint64_t)b * ntiles, last = first + ntiles - 1;
     totals[b] = tile_off[last] + tile_hist[last] - tile_off[first];
+    if (minhop_src) {  // hand the minimum hops over and reset them for the next histogram
+      minhop_dst[b] = minhop_src[b];
+      minhop_src[b] = 0xffffffffu;
+    }
+  }
+}
+
+__global__ void fetch_u64_pair_kernel(const uint64_t* src_a, uint64_t* __restrict__ dst_a,
+                                      const uint64_t* src_b, uint64_t* __restrict__ dst_b, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    dst_a[i] = src_a[i];
+    dst_b[i] = src_b[i];
   }
 }
 
@@ -129,13 +145,22 @@ cudaError_t launch_partition_hist(const gw_walk_rec* walks, const uint32_t* dest
 }
 
 cudaError_t launch_partition_scan(const uint32_t* tile_hist, uint32_t* tile_off, uint32_t* totals,
-                                  const PartitionPlan& plan, void* temp, cudaStream_t stream) {
+                                  const PartitionPlan& plan, void* temp, cudaStream_t stream,
+                                  uint32_t* minhop_src, uint32_t* minhop_dst) {
   size_t bytes = plan.scan_temp_bytes;
   cudaError_t e = cub::DeviceScan::ExclusiveSum(temp, bytes, tile_hist, tile_off,
                                                 (int64_t)plan.nbuckets * plan.ntiles, stream);
   if (e != cudaSuccess) return e;
   partition_totals_kernel<<<(plan.nbuckets + 255) / 256, 256, 0, stream>>>(
-      tile_hist, tile_off, plan.nbuckets, plan.ntiles, totals);
+      tile_hist, tile_off, plan.nbuckets, plan.ntiles, totals, minhop_src, minhop_dst);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fetch_u64_pair(const uint64_t* src_a, uint64_t* dst_a, const uint64_t* src_b,
+                                  uint64_t* dst_b, uint32_t n, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  const uint32_t grid = std::min<uint32_t>((n + 255) / 256, 64);
+  fetch_u64_pair_kernel<<<grid, 256, 0, stream>>>(src_a, dst_a, src_b, dst_b, n);
   return cudaGetLastError();
 }
 

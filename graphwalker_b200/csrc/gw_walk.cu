@@ -145,6 +145,9 @@ __global__ void __launch_bounds__(kWalkThreads)
   uint32_t st = 0, clos = 0;
   const L2Hints hp = make_hints(a.hints);
   DrawCache dc;
+  // the slice's first edge index (csr[0] is edge b0); read once, since the
+  // slice may be pinned host memory read over the host link
+  const unsigned long long b0 = SLICE && n ? __ldg(beg_pos) : 0ull;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     uint4 w = *(reinterpret_cast<const uint4*>(walks) + i);
     uint32_t v = w.x, id = w.y, src = w.z, hop = w.w;
@@ -171,7 +174,7 @@ __global__ void __launch_bounds__(kWalkThreads)
         break;
       }
       bool moved;
-      if (SLICE) moved = hop_advance_slice<RULE>(beg_pos, csr, a, id, src, hop, v, dc);
+      if (SLICE) moved = hop_advance_slice<RULE>(beg_pos, csr, b0, a, id, src, hop, v, dc);
       else moved = hop_advance<RULE>(g, a, hp, id, src, hop, v, dc);
       if (!moved) {
         ended = true;

@@ -173,6 +173,11 @@ class Graph:
         """Moves the CSR between HBM and pinned host memory (streamed blocks)."""
         check(load().gw_set_residency(self._h, residency, nmblocks), self._h)
 
+    def set_mapped_block_walks(self, max_walks: int) -> None:
+        """Streamed blocks with at most max_walks pending walks (and in no
+        device slot) are read in place from pinned host memory, not copied."""
+        check(load().gw_set_mapped_block_walks(self._h, max_walks), self._h)
+
     # ---- pools (WalkManager) ----
     def walks_clear(self) -> None:
         check(load().gw_walks_clear(self._h), self._h)

@@ -134,6 +134,9 @@ typedef struct gw_run_stats {
   double ms_walk;          /* of which walk kernels                          */
   double ms_partition;     /* of which pool partitioning                     */
   double ms_copy_wait;     /* of which waiting for block copies              */
+  uint64_t mapped_supersteps; /* block executions read in place from pinned
+                                 host memory (streaming, gw_set_mapped_block_walks) */
+  uint64_t mapped_walks;   /* walks those executions advanced                 */
 } gw_run_stats;
 
 /* ---- version / codec (host only, no device needed) -------------------- */
@@ -187,6 +190,16 @@ gw_status gw_export_csr(gw_ctx *ctx, uint64_t *rowptr, uint32_t *colidx);
    (GW_STREAM_PINNED, blocks streamed into `nmblocks` device slots, the
    reference's in-memory block budget, graphwalker.hpp:84-86).              */
 gw_status gw_set_residency(gw_ctx *ctx, uint32_t residency, uint32_t nmblocks);
+/* Streamed residency: a block the scheduler chooses that is in no device slot
+   and has at most `max_walks` pending walks is not copied into a slot; its
+   walks read the block's beg_pos and csr in place from pinned host memory over
+   the host link, a few sectors per hop instead of the whole block.  Which
+   block runs when is unchanged, and so are walks and counts.  0 copies every
+   block, as findSubGraph does (graphwalker.hpp:210-228); GW_MAPPED_AUTO (the
+   default) reads a block in place when it has at most one pending walk per
+   128 bytes of its CSR (beg_pos + csr slice).                              */
+#define GW_MAPPED_AUTO 0xFFFFFFFFFFFFFFFFull
+gw_status gw_set_mapped_block_walks(gw_ctx *ctx, uint64_t max_walks);
 
 /* ---- walk pools (WalkManager) ------------------------------------------- */
 gw_status gw_walks_clear(gw_ctx *ctx);

@@ -143,10 +143,22 @@ def test_config1_streamed_blocks_equal_oracle(config1, config1_oracle_counts):
         G.walks_clear()
         G.add_walks_at(np.arange(G.nv, dtype=np.uint32))
         G.set_residency(gw.STREAM_PINNED, nmblocks=8)
-        st = G.run(gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, L1, seed=SEED, mode=gw.MODE_BLOCKED, prob=0.2))
-        assert st.block_loads > 33  # blocks were evicted and loaded again
-        assert np.array_equal(G.read_counts(), config1_oracle_counts)
+        steps = None
+        # every chosen block copied into a slot (findSubGraph); blocks with at
+        # most 64 k pending walks read in place; the default per-block rule
+        for limit in (0, 1 << 16, gw.MAPPED_AUTO):
+            G.set_mapped_block_walks(limit)
+            st = G.run(gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, L1, seed=SEED, mode=gw.MODE_BLOCKED,
+                                 prob=0.2))
+            assert np.array_equal(G.read_counts(), config1_oracle_counts), limit
+            steps = steps or st.supersteps
+            assert st.supersteps == steps  # the same block order
+            if limit == 0:
+                assert st.block_loads > 33 and st.mapped_supersteps == 0  # blocks evicted and loaded again
+            else:
+                assert 0 < st.mapped_supersteps < st.supersteps
     finally:
+        G.set_mapped_block_walks(gw.MAPPED_AUTO)
         G.set_residency(gw.RESIDENT_HBM)
 
 

@@ -137,6 +137,7 @@ def test_blocked_engine_matches_reference_loop(cuda_device, oracle, case, prob):
         assert np.array_equal(ref["counts"], g[f"{tag}_counts"])
         for residency in (gw.RESIDENT_HBM, gw.STREAM_PINNED):
             with _graph(g, residency) as G:
+                G.set_mapped_block_walks(0)  # every block copied, as findSubGraph does
                 _add_golden_walks(G, g, tag)
                 st = G.run(gw.params(rule, gw.SINK_VERTEX_COUNT, L, seed=int(g["seed"]),
                                      mode=gw.MODE_BLOCKED, prob=prob))
@@ -144,6 +145,34 @@ def test_blocked_engine_matches_reference_loop(cuda_device, oracle, case, prob):
                 assert st.supersteps == ref["supersteps"]
                 if residency == gw.STREAM_PINNED:
                     assert st.block_loads >= 1
+
+
+@pytest.mark.parametrize("case", ["rmat10", "rmat13"])
+@pytest.mark.parametrize("mapped", ["all", "small"])
+def test_streamed_blocks_read_in_place_match_reference_loop(cuda_device, oracle, case, mapped):
+    """Streamed blocks whose pools are small are read in place from pinned host
+    memory instead of being copied into a slot: the same supersteps, the same
+    counts, and (every block read in place) no block copies at all."""
+    import graphwalker_b200 as gw
+    g = load_golden(case)
+    for tag in ("jump", "stop"):
+        rule, L = int(g[f"{tag}_rule"]), int(g[f"{tag}_L"])
+        ref = oracle.block_engine(g["rowptr"], g["colidx"], g["blocks"], g[f"{tag}_cur"], rule=rule, L=L,
+                                  seed=int(g["seed"]), prob=0.2)
+        limit = (1 << 63) if mapped == "all" else max(1, len(g[f"{tag}_cur"]) // (4 * (len(g["blocks"]) - 1)))
+        with _graph(g, gw.STREAM_PINNED) as G:
+            G.set_mapped_block_walks(limit)
+            _add_golden_walks(G, g, tag)
+            st = G.run(gw.params(rule, gw.SINK_VERTEX_COUNT, L, seed=int(g["seed"]), mode=gw.MODE_BLOCKED,
+                                 prob=0.2))
+            assert np.array_equal(G.read_counts(), g[f"{tag}_counts"]), f"{case}/{tag}/{mapped}"
+            assert st.supersteps == ref["supersteps"]
+            assert st.mapped_supersteps >= 1
+            if mapped == "all":
+                assert st.block_loads == 0 and st.bytes_h2d == 0
+                assert st.mapped_supersteps == st.supersteps and st.mapped_walks >= len(g[f"{tag}_cur"])
+            else:
+                assert st.mapped_supersteps < st.supersteps
 
 
 @pytest.mark.parametrize("steps", [1, 3, 7])
