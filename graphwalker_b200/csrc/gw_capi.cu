@@ -102,7 +102,10 @@ gw_status apply_edge_records(gw_ctx* ctx) {
 }
 
 // Uploads the CSR (host pointers, pinned or not) and builds the packed
-// vertex records; keeps a pinned host copy for streamed residency.
+// vertex records.  Streamed residency keeps the CSR in pinned host memory and
+// only the row pointer (8 bytes per vertex) in HBM: blocks then stream their
+// column slices alone, and a block read in place fetches only its columns
+// over the host link.
 gw_status install_graph(gw_ctx* ctx, const uint64_t* rowptr, const uint32_t* colidx,
                         uint32_t nv, const uint32_t* blocks, uint32_t nblocks) {
   ctx->nv = nv;
@@ -128,6 +131,9 @@ gw_status install_graph(gw_ctx* ctx, const uint64_t* rowptr, const uint32_t* col
       GW_CUDA(ctx, ctx->h_colidx.ensure(ci_bytes), "pinned colidx");
       memcpy(ctx->h_colidx.p, colidx, ci_bytes);
     }
+    GW_CUDA(ctx, ctx->d_rowptr.ensure(rp_bytes), "rowptr alloc");
+    GW_CUDA(ctx, cudaMemcpyAsync(ctx->d_rowptr.p, ctx->h_rowptr.p, rp_bytes, cudaMemcpyHostToDevice,
+                                 ctx->stream), "rowptr copy");
   } else {
     GW_CUDA(ctx, ctx->d_rowptr.ensure(rp_bytes), "rowptr alloc");
     GW_CUDA(ctx, ctx->d_colidx.ensure(ci_bytes), "colidx alloc");
@@ -530,8 +536,7 @@ gw_status gw_set_residency(gw_ctx* ctx, uint32_t residency, uint32_t nmblocks) {
     GW_CUDA(ctx, ctx->h_colidx.ensure(ci), "pinned colidx");
     GW_CUDA(ctx, cudaMemcpy(ctx->h_rowptr.p, ctx->d_rowptr.p, rp, cudaMemcpyDeviceToHost), "rowptr to host");
     if (ci) GW_CUDA(ctx, cudaMemcpy(ctx->h_colidx.p, ctx->d_colidx.p, ci, cudaMemcpyDeviceToHost), "colidx to host");
-    ctx->d_rowptr.release();
-    ctx->d_colidx.release();
+    ctx->d_colidx.release();  // the row pointer stays in HBM
     ctx->d_vrec.release();
     ctx->d_erec.release();
   } else {

@@ -18,10 +18,11 @@
 //
 // Streaming differs from findSubGraph in two ways that change neither the
 // order of blocks nor any walk:
+//  * the row pointer stays in HBM, and a slot holds a block's column slice;
 //  * a chosen block in no slot whose pool is small (ctx->mapped_max_walks,
-//    or per block its CSR bytes / kMappedBytesPerWalk) is read in place from
-//    the pinned host copy through its mapped device address: its walks fetch
-//    a few sectors per hop over the host link instead of the whole block;
+//    or per block its column bytes / kMappedBytesPerWalk) is read in place
+//    from the pinned host columns through their mapped device address: each
+//    hop fetches one sector over the host link instead of the whole block;
 //  * while a block runs, up to kCopyAhead blocks with many pending walks are
 //    copied into slots before their turn, each taking the room of the slot
 //    with the fewest pending walks (swapOut's victim) when it has more.
@@ -36,24 +37,24 @@ namespace {
 
 constexpr uint32_t kNoBlock = 0xffffffffu;
 // GW_MAPPED_AUTO: a streamed block runs in place when it has at most one
-// pending walk per this many bytes of its CSR.  Copying a block costs its
-// bytes at the host link's rate; a walk run in place costs a few sectors
-// fetched over the same link and waits on their latency.
+// pending walk per this many bytes of its column slice.  Copying a block
+// costs its bytes at the host link's rate; a walk run in place costs a sector
+// per hop fetched over the same link and waits on its latency.
 constexpr uint64_t kMappedBytesPerWalk = 128;
 // Blocks copied ahead of their turn at most (1 to 5 measured within 2 % of
 // one another on an out-of-core scale-27 graph, the deeper the faster).
 constexpr size_t kCopyAhead = 3;
 
 struct Slots {
-  // One device slot holds the CSR slice of one block:
-  //   beg_pos[blocks[b] .. blocks[b+1]] and csr[beg_pos[blocks[b]] .. beg_pos[blocks[b+1]]).
-  std::vector<gw_devbuf> beg_pos, csr;
+  // One device slot holds the column slice of one block,
+  //   csr[beg_pos[blocks[b]] .. beg_pos[blocks[b+1]]);
+  // the row pointer of every block stays in HBM.
+  std::vector<gw_devbuf> csr;
   std::vector<uint32_t> block;      // block held, kNoBlock if empty
   std::vector<cudaEvent_t> ready;   // copy finished
   std::vector<cudaEvent_t> free_ev; // last kernel reading the slot finished
   std::vector<int> slot_of;         // per block: slot index or -1
   ~Slots() {
-    for (auto& b : beg_pos) b.release();
     for (auto& b : csr) b.release();
     for (auto e : ready) cudaEventDestroy(e);
     for (auto e : free_ev) cudaEventDestroy(e);
@@ -185,44 +186,34 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
   Slots slots;
   const uint32_t nslots = streaming ? std::max<uint32_t>(2, std::min(ctx->nmblocks, nb)) : 0;
   if (streaming) {
-    uint64_t max_v = 0, max_e = 0;
+    uint64_t max_e = 0;
     const uint64_t* hr = ctx->h_rowptr.as<uint64_t>();
-    for (uint32_t b = 0; b < nb; ++b) {
-      max_v = std::max<uint64_t>(max_v, ctx->blocks[b + 1] - ctx->blocks[b]);
-      max_e = std::max<uint64_t>(max_e, hr[ctx->blocks[b + 1]] - hr[ctx->blocks[b]]);
-    }
-    slots.beg_pos.resize(nslots);
+    for (uint32_t b = 0; b < nb; ++b) max_e = std::max<uint64_t>(max_e, hr[ctx->blocks[b + 1]] - hr[ctx->blocks[b]]);
     slots.csr.resize(nslots);
     slots.block.assign(nslots, kNoBlock);
     slots.ready.resize(nslots);
     slots.free_ev.resize(nslots);
     slots.slot_of.assign(nb, -1);
     for (uint32_t i = 0; i < nslots; ++i) {
-      GW_CUDA(ctx, slots.beg_pos[i].ensure((max_v + 1) * 8), "slot alloc");
       GW_CUDA(ctx, slots.csr[i].ensure(std::max<uint64_t>(max_e, 1) * 4), "slot alloc");
       cudaEventCreateWithFlags(&slots.ready[i], cudaEventDisableTiming);
       cudaEventCreateWithFlags(&slots.free_ev[i], cudaEventDisableTiming);
       cudaEventRecord(slots.free_ev[i], st);
     }
   }
-  // mapped device addresses of the pinned host CSR (blocks read in place)
-  const unsigned long long* m_rowptr = nullptr;
+  // mapped device address of the pinned host columns (blocks read in place)
   const uint32_t* m_colidx = nullptr;
   if (streaming && ctx->mapped_max_walks) {
     void* mp = nullptr;
-    GW_CUDA(ctx, cudaHostGetDevicePointer(&mp, ctx->h_rowptr.p, 0), "mapped rowptr");
-    m_rowptr = static_cast<const unsigned long long*>(mp);
     GW_CUDA(ctx, cudaHostGetDevicePointer(&mp, ctx->h_colidx.p, 0), "mapped colidx");
     m_colidx = static_cast<const uint32_t*>(mp);
   }
   // the most pending walks at which block q runs in place (0 = never)
   auto mapped_limit = [&](uint32_t q) -> uint64_t {
-    if (!m_rowptr) return 0;
+    if (!m_colidx) return 0;
     if (ctx->mapped_max_walks != GW_MAPPED_AUTO) return ctx->mapped_max_walks;
     const uint64_t* hr = ctx->h_rowptr.as<uint64_t>();
-    const uint64_t bytes = ((uint64_t)ctx->blocks[q + 1] - ctx->blocks[q] + 1) * 8 +
-                           (hr[ctx->blocks[q + 1]] - hr[ctx->blocks[q]]) * 4;
-    return bytes / kMappedBytesPerWalk;
+    return (hr[ctx->blocks[q + 1]] - hr[ctx->blocks[q]]) * 4 / kMappedBytesPerWalk;
   };
   ctx->stats = gw_run_stats{};
   ctx->stats.walks = nwalks;
@@ -251,8 +242,6 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     const uint32_t v0 = ctx->blocks[b], v1 = ctx->blocks[b + 1];
     const uint64_t e0 = hr[v0], e1 = hr[v1];
     cudaStreamWaitEvent(xs, slots.free_ev[victim], 0);
-    cudaMemcpyAsync(slots.beg_pos[victim].p, hr + v0, ((uint64_t)v1 - v0 + 1) * 8,
-                    cudaMemcpyHostToDevice, xs);
     if (e1 > e0)
       cudaMemcpyAsync(slots.csr[victim].p, ctx->h_colidx.as<uint32_t>() + e0, (e1 - e0) * 4,
                       cudaMemcpyHostToDevice, xs);
@@ -260,7 +249,7 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     slots.block[victim] = b;
     slots.slot_of[b] = victim;
     ctx->stats.block_loads++;
-    ctx->stats.bytes_h2d += ((uint64_t)v1 - v0 + 1) * 8 + (e1 - e0) * 4;
+    ctx->stats.bytes_h2d += (e1 - e0) * 4;
     return victim;
   };
 
@@ -342,16 +331,14 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     cudaEventRecord(ph[0], st);
     if (streaming) {
       ahead.erase(std::remove(ahead.begin(), ahead.end(), b), ahead.end());
+      beg_pos = ctx->d_rowptr.as<unsigned long long>() + ab.lo;
       if (slots.slot_of[b] < 0 && n <= mapped_limit(b)) {
-        const uint64_t e0 = ctx->h_rowptr.as<uint64_t>()[ab.lo];
-        beg_pos = m_rowptr + ab.lo;
-        csr = m_colidx + e0;
+        csr = m_colidx + ctx->h_rowptr.as<uint64_t>()[ab.lo];
         ctx->stats.mapped_supersteps++;
         ctx->stats.mapped_walks += n;
       } else {
         slot = load_block(b, -1);
         cudaStreamWaitEvent(st, slots.ready[slot], 0);
-        beg_pos = slots.beg_pos[slot].as<unsigned long long>();
         csr = slots.csr[slot].as<uint32_t>();
       }
     }

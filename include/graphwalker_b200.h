@@ -188,7 +188,9 @@ gw_status gw_get_blocks(gw_ctx *ctx, uint32_t *blocks, uint32_t cap);
 gw_status gw_export_csr(gw_ctx *ctx, uint64_t *rowptr, uint32_t *colidx);
 /* Moves the CSR between HBM (GW_RESIDENT_HBM) and pinned host memory
    (GW_STREAM_PINNED, blocks streamed into `nmblocks` device slots, the
-   reference's in-memory block budget, graphwalker.hpp:84-86).              */
+   reference's in-memory block budget, graphwalker.hpp:84-86).  Streamed, the
+   row pointer (8 bytes per vertex) stays in HBM and a slot holds one block's
+   column slice.                                                             */
 gw_status gw_set_residency(gw_ctx *ctx, uint32_t residency, uint32_t nmblocks);
 /* Streamed residency: a block the scheduler chooses that is in no device slot
    and has at most `max_walks` pending walks is not copied into a slot; its
@@ -197,7 +199,7 @@ gw_status gw_set_residency(gw_ctx *ctx, uint32_t residency, uint32_t nmblocks);
    block runs when is unchanged, and so are walks and counts.  0 copies every
    block, as findSubGraph does (graphwalker.hpp:210-228); GW_MAPPED_AUTO (the
    default) reads a block in place when it has at most one pending walk per
-   128 bytes of its CSR (beg_pos + csr slice).                              */
+   128 bytes of its column slice.                                            */
 #define GW_MAPPED_AUTO 0xFFFFFFFFFFFFFFFFull
 gw_status gw_set_mapped_block_walks(gw_ctx *ctx, uint64_t max_walks);
 
