@@ -128,6 +128,8 @@ _SIGS = {
     "gw_read_stats": (c_int32, [_P, POINTER(RunStats)]),
     "gw_read_pool": (c_int32, [_P, c_uint32, _P, c_size_t, POINTER(c_uint64)]),
     "gw_run_pools": (c_int32, [_P, POINTER(WalkParams), _P, _P, _P, _P]),
+    "gw_run_pools_submit": (c_int32, [_P, POINTER(WalkParams), _P, _P, _P, _P, POINTER(c_uint64)]),
+    "gw_run_pools_wait": (c_int32, [_P, c_uint64]),
     "gw_walk_device": (c_int32, [_P, POINTER(WalkParams), _P, c_uint64, _P, _P, _P, _P, _P]),
     "gw_unpack_words_device": (c_int32, [_P, c_uint32, _P, _P, c_uint64, _P, _P]),
     "gw_pack_words_device": (c_int32, [_P, _P, c_uint64, _P, _P, _P]),

@@ -472,6 +472,7 @@ gw_status gw_close(gw_ctx* ctx) {
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   if (ctx->aux_stream) cudaStreamSynchronize(ctx->aux_stream);
   if (ctx->l2_persist_bytes) gw_set_l2_persisting(ctx, 0);
+  gw::pipe_release(ctx);
   for (gw_devbuf* b : {&ctx->d_rowptr, &ctx->d_colidx, &ctx->d_vrec, &ctx->d_erec, &ctx->d_meet, &ctx->d_sr_rows, &ctx->d_blocks,
                        &ctx->d_status,
                        &ctx->d_walks, &ctx->d_words, &ctx->d_ids, &ctx->d_counts, &ctx->d_paths,

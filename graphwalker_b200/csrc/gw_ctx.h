@@ -111,6 +111,20 @@ struct gw_ctx {
   // L2 persisting reservation for the visit counters (0 = none)
   uint64_t l2_persist_bytes = 0;
 
+  // gw_run_pools_submit / gw_run_pools_wait: two runs in flight, each with
+  // its own device buffers, status word and events (slot = ticket & 1).
+  struct PoolsPipe {
+    gw_devbuf walks[2], words[2], ids[2], offsets[2], counts[2], status[2];
+    gw_hostbuf h_status;                 // 2 words, pinned
+    cudaEvent_t run_done[2] = {};        // the run's walks finished
+    cudaEvent_t out_done[2] = {};        // its counts and status are on the host
+    cudaEvent_t start[2] = {};           // the run's counters are clear
+    cudaStream_t readback = nullptr;     // device-to-host copies of finished runs
+    uint64_t next_ticket = 1;
+    uint64_t ticket[2] = {0, 0};         // ticket held by the slot (0 = free)
+    bool waited[2] = {true, true};
+  } pipe;
+
   // multi-source PPR queries
   gw_devbuf d_q_sources, d_q_prefix, d_q_idbase, d_q_toff, d_q_tmask, d_q_tables, d_q_full, d_q_ids,
       d_q_counts, d_q_visits, d_q_cursor, d_q_segs, d_q_cand;
@@ -181,6 +195,8 @@ gw_status read_status(gw_ctx* ctx);
 gw_status status_of(gw_ctx* ctx, uint32_t bits);
 // GraphWalker's block loop on the device (gw_engine.cu).
 gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p);
+// Frees the buffers, events and stream of gw_run_pools_submit (gw_pools_async.cu).
+void pipe_release(gw_ctx* ctx);
 }  // namespace gw
 
 #define GW_CUDA(ctx, expr, what)                    \

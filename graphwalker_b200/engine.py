@@ -247,6 +247,19 @@ class Graph:
         check(load().gw_run_pools(self._h, byref(p), _ptr(words), _ptr(pool_offsets), _ptr(ids),
                                   _ptr(counts_out)), self._h)
 
+    def run_pools_submit(self, p: WalkParams, words: np.ndarray, pool_offsets: np.ndarray,
+                         counts_out: np.ndarray, ids: np.ndarray | None = None) -> int:
+        """Queues a run_pools (gw_run_pools_submit) and returns its ticket; the
+        arrays must stay alive, and counts_out unread, until run_pools_wait."""
+        t = c_uint64(0)
+        check(load().gw_run_pools_submit(self._h, byref(p), _ptr(words), _ptr(pool_offsets), _ptr(ids),
+                                         _ptr(counts_out), byref(t)), self._h)
+        return int(t.value)
+
+    def run_pools_wait(self, ticket: int) -> None:
+        """Blocks until the run of `ticket` has its counts on the host."""
+        check(load().gw_run_pools_wait(self._h, ticket), self._h)
+
     # ---- device-pointer entry points ----
     def walk_device(self, p: WalkParams, walks, n: int, counts=None, paths=None, plen=None,
                     closure=None, stream: int | None = None) -> None:

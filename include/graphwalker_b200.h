@@ -232,6 +232,20 @@ gw_status gw_read_pool(gw_ctx *ctx, uint32_t block, gw_walk_rec *out, size_t cap
    (VERTEX_COUNT sink; counts is overwritten).  ids may be NULL.            */
 gw_status gw_run_pools(gw_ctx *ctx, const gw_walk_params *params, const uint64_t *words,
                        const uint64_t *pool_offsets, const uint32_t *ids, uint32_t *counts);
+/* gw_run_pools in two halves, so that back-to-back runs overlap.  submit
+   queues one run (the copy of the words in, the walks, the copy of the counts
+   out to `counts`) and returns its ticket; wait blocks until that run's counts
+   are in `counts` and returns the run's status.  Two runs can be in flight: a
+   third submit fails with GW_E_STATE until the older one is waited on.  Each
+   run in flight has its own device words, walks, counters and status word,
+   so a run's count read-back overlaps the next run's copies and walks.
+   words, pool_offsets, ids and counts must stay valid, and counts unread,
+   until the wait returns; pinned host memory keeps the copies asynchronous.
+   The counts equal gw_run_pools's for the same arguments.                  */
+gw_status gw_run_pools_submit(gw_ctx *ctx, const gw_walk_params *params, const uint64_t *words,
+                              const uint64_t *pool_offsets, const uint32_t *ids, uint32_t *counts,
+                              uint64_t *ticket);
+gw_status gw_run_pools_wait(gw_ctx *ctx, uint64_t ticket);
 
 /* ---- multi-source PPR queries (msppr, apps/msppr.cpp:25-145) ------------ */
 typedef struct gw_ppr_stats {

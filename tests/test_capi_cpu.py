@@ -145,11 +145,27 @@ def test_close_releases_every_context_buffer():
     ctx_h = (ROOT / "graphwalker_b200" / "csrc" / "gw_ctx.h").read_text()
     body = re.search(r"struct gw_ctx \{(.*?)\n\};", ctx_h, re.S).group(1)
     code = "\n".join(line.split("//")[0] for line in body.splitlines())
-    held = set()
-    for decl in re.findall(r"\bgw_(?:dev|host)buf\s+([^;(){}]*);", code):
-        held |= {name.strip() for name in decl.split(",")}
+    # the submit/wait pipeline's buffers live in a nested struct, freed by
+    # gw::pipe_release, which gw_close calls
+    pipe = re.search(r"struct PoolsPipe \{(.*?)\} pipe;", code, re.S)
+    code = code.replace(pipe.group(0), "")
+
+    def buffers(text):
+        held = set()
+        for decl in re.findall(r"\bgw_(?:dev|host)buf\s+([^;(){}]*);", text):
+            held |= {name.split("[")[0].strip() for name in decl.split(",")}
+        return held
+
+    held = buffers(code)
     capi = (ROOT / "graphwalker_b200" / "csrc" / "gw_capi.cu").read_text()
     start = capi.index("gw_status gw_close(gw_ctx* ctx)")
     close = capi[start:capi.index("\n}\n", start)]
     named = set(re.findall(r"ctx->(\w+)", close))
     assert held and held <= named, sorted(held - named)
+    assert "gw::pipe_release(ctx)" in close
+    src = (ROOT / "graphwalker_b200" / "csrc" / "gw_pools_async.cu").read_text()
+    start = src.index("void pipe_release(gw_ctx* ctx)")
+    release = src[start:src.index("\n}\n", start)]
+    held_pipe = buffers(pipe.group(1))
+    named_pipe = set(re.findall(r"P\.(\w+)", release))
+    assert held_pipe and held_pipe <= named_pipe, sorted(held_pipe - named_pipe)

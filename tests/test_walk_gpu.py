@@ -244,6 +244,57 @@ def test_run_pools_host_call(cuda_device, oracle):
         assert np.array_equal(out, ref["counts"])
 
 
+def test_run_pools_pipelined_equals_oracle(cuda_device, oracle):
+    """gw_run_pools_submit / wait: two runs in flight, each with the counts of
+    its own seed (and ids); a third submit is refused until the older run is
+    waited on; a device error reaches the wait of its own run only."""
+    import graphwalker_b200 as gw
+    from graphwalker_b200._lib import GW_E_BOUNDS, GW_E_INVALID, GW_E_STATE, GwError
+    rp, ci = oracle.rmat_csr(15, 16, seed=4)
+    blocks = oracle.compute_blocks(rp, 256)
+    nv = len(rp) - 1
+    cur = np.arange(nv, dtype=np.uint32)
+    blk = np.searchsorted(blocks[1:], cur, side="right")
+    words = gw.encode(cur, cur - blocks[blk], 0)
+    offs = np.r_[0, np.cumsum(np.bincount(blk, minlength=len(blocks) - 1))].astype(np.uint64)
+    ids = (cur * 7 + 11).astype(np.uint32)
+    seeds = [3, 4, 5, 6, 7]
+    refs = {s: oracle.run_walks(rp, ci, cur, ids=ids if s % 2 else None, rule=0, L=10, seed=s)["counts"]
+            for s in seeds}
+    with gw.Graph.from_csr(rp, ci, blocks) as G:
+        outs = {s: np.full(nv, 0xDEAD, np.uint32) for s in seeds}
+        pending = []
+        for s in seeds:
+            if len(pending) == 2:
+                with pytest.raises(GwError) as e:  # two in flight already
+                    G.run_pools_submit(gw.params(0, gw.SINK_VERTEX_COUNT, 10, seed=s), words, offs, outs[s])
+                assert e.value.code == GW_E_STATE
+                t, done = pending.pop(0)
+                G.run_pools_wait(t)
+                assert np.array_equal(outs[done], refs[done]), done
+            t = G.run_pools_submit(gw.params(0, gw.SINK_VERTEX_COUNT, 10, seed=s), words, offs, outs[s],
+                                   ids=ids if s % 2 else None)
+            pending.append((t, s))
+        for t, done in pending:
+            G.run_pools_wait(t)
+            assert np.array_equal(outs[done], refs[done]), done
+        with pytest.raises(GwError) as e:
+            G.run_pools_wait(pending[-1][0])  # already waited
+        assert e.value.code == GW_E_INVALID
+        # a walk past the last vertex: its run's wait reports GW_E_BOUNDS, the
+        # run in flight beside it is unaffected
+        bad = words.copy()
+        bad[-1] = gw.encode([0], [nv - int(blocks[-2]) + 5], [0])[0]
+        out_bad, out_ok = np.zeros(nv, np.uint32), np.zeros(nv, np.uint32)
+        tb = G.run_pools_submit(gw.params(0, gw.SINK_VERTEX_COUNT, 10, seed=3), bad, offs, out_bad)
+        tk = G.run_pools_submit(gw.params(0, gw.SINK_VERTEX_COUNT, 10, seed=4), words, offs, out_ok)
+        with pytest.raises(GwError) as e:
+            G.run_pools_wait(tb)
+        assert e.value.code == GW_E_BOUNDS
+        G.run_pools_wait(tk)
+        assert np.array_equal(out_ok, refs[4])
+
+
 def test_errors_surface_as_status_codes(cuda_device, oracle):
     import graphwalker_b200 as gw
     from graphwalker_b200._lib import GW_E_BOUNDS, GW_E_INVALID, GW_E_OVERFLOW, GwError
