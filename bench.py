@@ -92,6 +92,10 @@ def parse_args():
                          "(small profiler captures)")
     ap.add_argument("--probe-mb", type=int, default=2048, help="gather: buffer size")
     ap.add_argument("--probe-loads", type=int, default=1 << 26, help="gather: loads per launch")
+    ap.add_argument("--probe-host", action="store_true",
+                    help="gather: the buffer in pinned host memory, read by the kernel over the host link")
+    ap.add_argument("--mapped-walks", default="auto",
+                    help="ooc: gw_set_mapped_block_walks of the default streamed run ('auto' or a number)")
     ap.add_argument("--rng", choices=["philox", "native"], default="philox", help="walkonly: random stream")
     ap.add_argument("--hints", type=int, default=-1,
                     help="walkonly: explicit GW_HINT_* bits for the walk kernel (-1: the engine default)")
@@ -974,7 +978,8 @@ def ooc_measure(args) -> dict:
                 ("resident_one_launch", gw.RESIDENT_HBM, gw.MODE_RESIDENT, gw.MAPPED_AUTO),
                 ("resident_blocked", gw.RESIDENT_HBM, gw.MODE_BLOCKED, gw.MAPPED_AUTO),
                 ("streamed_blocked_copy_all", gw.STREAM_PINNED, gw.MODE_BLOCKED, 0),
-                ("streamed_blocked", gw.STREAM_PINNED, gw.MODE_BLOCKED, gw.MAPPED_AUTO)):
+                ("streamed_blocked", gw.STREAM_PINNED, gw.MODE_BLOCKED,
+                 gw.MAPPED_AUTO if args.mapped_walks == "auto" else int(args.mapped_walks))):
             G.set_residency(residency, nmblocks=slots)
             G.set_mapped_block_walks(mapped)
             st = G.run(gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, L, seed=args.walk_seed, mode=mode, prob=0.2))
@@ -1002,7 +1007,8 @@ def ooc_measure(args) -> dict:
                 "dtype": "u32", "data": "synthetic",
                 "config": {"workload": f"out-of-core raw random walks, R-MAT scale {scale} ef {ef}, {G.nblocks} blocks "
                                        f"in pinned host memory, {slots} device block slots, one walk per vertex, "
-                                       f"L={L}, jump rule", "graph_GB": graph_bytes / 1e9, "generate_s": gen_s},
+                                       f"L={L}, jump rule", "graph_GB": graph_bytes / 1e9, "generate_s": gen_s,
+                           "in_place_limit": args.mapped_walks},
                 "host_link_GBps": link, "modes": res, "identical_counts_across_modes": same,
                 "speedup_vs_copy_all": res["streamed_blocked_copy_all"]["ms"] / s["ms"]}
     finally:
@@ -1201,10 +1207,14 @@ def gather_arm(args) -> None:
     import graphwalker_b200 as gw
     torch.cuda.set_device(0)
     with gw.Graph.rmat(10, 4, seed=1, blocksize_kb=64) as G:
-        buf = torch.zeros(args.probe_mb << 18, dtype=torch.int32, device="cuda")
-        bps = G.probe_gather(buf, buf.numel(), args.probe_loads, iters=2)
+        if args.probe_host:  # pinned host memory: its address is valid on the device
+            buf = torch.zeros(args.probe_mb << 18, dtype=torch.int32).pin_memory()
+        else:
+            buf = torch.zeros(args.probe_mb << 18, dtype=torch.int32, device="cuda")
+        bps = G.probe_gather(buf.data_ptr(), buf.numel(), args.probe_loads, iters=2)
     print(json.dumps({"workload": "gather", "buffer_MB": args.probe_mb, "loads": args.probe_loads,
-                      "useful_GBps_32B": bps / 1e9}), flush=True)
+                      "memory": "pinned host" if args.probe_host else "device",
+                      "useful_GBps_32B": bps / 1e9, "loads_per_s": bps / 32}), flush=True)
 
 
 def walkonly_arm(args) -> None:
