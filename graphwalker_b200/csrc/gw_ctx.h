@@ -28,6 +28,14 @@ struct gw_devbuf {
     if (e == cudaSuccess) bytes = n;
     return e;
   }
+  // ensure() for a buffer whose need creeps up call after call: a growth
+  // takes at least half again the current size, so a run of slowly growing
+  // needs reallocates (and synchronises the device in cudaFree) a few times,
+  // not once per call.
+  cudaError_t grow(size_t n) {
+    if (n <= bytes && p) return cudaSuccess;
+    return ensure(n > bytes + bytes / 2 ? n : bytes + bytes / 2);
+  }
   void release() {
     if (p) cudaFree(p);
     p = nullptr;

@@ -323,10 +323,10 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
       e = cudaStreamSynchronize(st);
       if (e != cudaSuccess) break;
     }
-    GW_CUDA(ctx, ctx->d_dest.ensure(n * 4), "dest alloc");
-    GW_CUDA(ctx, ctx->d_tile_hist.ensure(hist_n * 4), "hist alloc");
-    GW_CUDA(ctx, ctx->d_tile_off.ensure(hist_n * 4), "hist alloc");
-    GW_CUDA(ctx, ctx->d_scan_temp.ensure(plan.scan_temp_bytes), "scan alloc");
+    GW_CUDA(ctx, ctx->d_dest.grow(n * 4), "dest alloc");
+    GW_CUDA(ctx, ctx->d_tile_hist.grow(hist_n * 4), "hist alloc");
+    GW_CUDA(ctx, ctx->d_tile_off.grow(hist_n * 4), "hist alloc");
+    GW_CUDA(ctx, ctx->d_scan_temp.grow(plan.scan_temp_bytes), "scan alloc");
     cudaEvent_t* ph = phase_set(superstep);
     cudaEventRecord(ph[0], st);
     if (streaming) {
