@@ -89,6 +89,38 @@ def test_compat_program_matches_reference_goldens(cuda_device, case, tmp_path):
         assert closure == int(g[f"{tag}_closure"])
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("mapped", ["0", "auto", "1000000"])
+def test_compat_streamed_block_loop_counts(cuda_device, mapped, tmp_path):
+    """The knobs of the streamed block loop through the drop-in engine
+    (gw_mode blocked, gw_residency stream, gw_mapped_walks, gw_sink count):
+    the program's counts equal the reference engine's goldens whether blocks
+    are copied into slots or read in place."""
+    g = load_golden("rmat13")
+    base = _prepare(tmp_path, g, "rmat13")
+    nv = len(g["rowptr"]) - 1
+    app = build_compat_app(0, tmp_path / "app0")
+    for tag in golden_runs(g):
+        if int(g[f"{tag}_rule"]) != 0:
+            continue
+        _walks_file(tmp_path / "walks.bin", g, tag)
+        out = tmp_path / "out.bin"
+        r = subprocess.run([str(app), base, str(int(g["blocksize_kb"])), str(tmp_path / "walks.bin"), str(out),
+                            str(int(g[f"{tag}_L"])), str(int(g["seed"])), str(nv), "1", "1",
+                            "gw_walk_id", "source", "seed", str(int(g["seed"])), "gw_mode", "blocked",
+                            "gw_residency", "stream", "gw_mapped_walks", mapped, "gw_sink", "count"],
+                           cwd=tmp_path, capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr[-2000:]
+        counts = np.frombuffer(out.read_bytes(), np.uint32, nv, 8)
+        assert np.array_equal(counts, g[f"{tag}_counts"]), f"{tag}/{mapped}"
+        metrics = "".join(p.read_text() for p in tmp_path.glob("*metrics.txt"))
+        in_place = int(float(re.search(r"gpu_blocks_read_in_place\D*?([\d.]+)", metrics).group(1)))
+        if mapped == "0":
+            assert in_place == 0, metrics[-500:]
+        elif mapped == "1000000":  # every block in place: none is ever copied
+            assert in_place > 0, metrics[-500:]
+
+
 def _run_app(app: str, args: list[str], cwd: Path) -> subprocess.CompletedProcess:
     exe = APPS_DIR / app
     if not exe.exists():
