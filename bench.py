@@ -94,6 +94,8 @@ def parse_args():
     ap.add_argument("--probe-loads", type=int, default=1 << 26, help="gather: loads per launch")
     ap.add_argument("--probe-host", action="store_true",
                     help="gather: the buffer in pinned host memory, read by the kernel over the host link")
+    ap.add_argument("--sink", choices=["count", "none"], default="count",
+                    help="walkonly: count visits per vertex (the headline's sink) or record nothing")
     ap.add_argument("--mapped-walks", default="auto",
                     help="ooc: gw_set_mapped_block_walks of the default streamed run ('auto' or a number)")
     ap.add_argument("--rng", choices=["philox", "native"], default="philox", help="walkonly: random stream")
@@ -483,11 +485,13 @@ def our_arm(args) -> None:
     last_counts = counts.cpu().numpy().view(np.uint32).copy() if world == 1 else None
 
     # random-sector gather roof: an 8 GB buffer, far larger than L2
-    gather_bps = None
+    gather_bps = red_ops_s = None
     if rank == 0 and not args.no_probe:
         buf = torch.empty(1 << 31, dtype=torch.int32, device="cuda")
         gather_bps = G.probe_gather(buf, buf.numel(), 1 << 28, iters=5)
         del buf
+        # and the visit-counter roof: one red.add per visit into nv counters
+        red_ops_s = G.probe_red(counts, nv, steps_per_launch, iters=5)
         torch.cuda.empty_cache()
 
     # e2e through the C-ABI host call (pinned words in, counts out)
@@ -545,6 +549,15 @@ def our_arm(args) -> None:
             roof["probe_dram_gbs"] = gather_bps / 1e9 * amp
             roof["line_fill_frac"] = roof["dram_gbs"] / roof["probe_dram_gbs"]
             roof["dram_bytes_per_step"] = traffic / steps_per_launch
+            if red_ops_s:
+                # the two resources a launch uses, each at its own probe's rate:
+                # its line fills (DRAM) and its visit-counter updates (L2 atomics)
+                fills_ms = traffic / (roof["probe_dram_gbs"] * 1e9) * 1e3
+                reds_ms = steps_per_launch / red_ops_s * 1e3
+                roof["counter_updates_per_s_probe"] = red_ops_s
+                roof["fills_alone_ms"] = fills_ms
+                roof["counter_updates_alone_ms"] = reds_ms
+                roof["fills_plus_updates_frac"] = (fills_ms + reds_ms) / kern_ms
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
             "warmup": max(3, args.warmup), "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
@@ -1238,8 +1251,8 @@ def walkonly_arm(args) -> None:
         walks = torch.stack([v, v, v, torch.zeros_like(v)], 1).to(torch.int32).contiguous()
         del v
         counts = torch.zeros(nv, dtype=torch.int32, device="cuda")
-        p = gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, args.L, seed=args.walk_seed,
-                      rng=gw.RNG_NATIVE if args.rng == "native" else gw.RNG_PHILOX,
+        p = gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT if args.sink == "count" else gw.SINK_NONE, args.L,
+                      seed=args.walk_seed, rng=gw.RNG_NATIVE if args.rng == "native" else gw.RNG_PHILOX,
                       cache_hints=None if args.hints < 0 else args.hints)
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(max(1, args.steps))]
@@ -1251,7 +1264,7 @@ def walkonly_arm(args) -> None:
         G.sync()
         visits = int(counts.to(torch.int64).sum().item())
     print(json.dumps({"workload": "walkonly", "scale": args.scale, "graph_layout": layout, "rng": args.rng,
-                      "hints": args.hints,
+                      "hints": args.hints, "sink": args.sink,
                       "launch_ms": [a.elapsed_time(b) for a, b in ev], "visits": visits}), flush=True)
 
 

@@ -135,6 +135,7 @@ _SIGS = {
     "gw_pack_words_device": (c_int32, [_P, _P, c_uint64, _P, _P, _P]),
     "gw_sync": (c_int32, [_P, _P]),
     "gw_probe_gather": (c_int32, [_P, _P, c_uint64, c_uint64, ctypes.c_int, POINTER(c_double)]),
+    "gw_probe_red": (c_int32, [_P, _P, c_uint64, c_uint64, ctypes.c_int, POINTER(c_double)]),
     "gw_superstep_static": (c_int32, [_P, POINTER(WalkParams), c_uint32, _P, c_uint64, _P, _P, _P, _P, _P]),
     "gw_ppr_run": (c_int32, [_P, POINTER(WalkParams), _P, _P, c_uint32, c_uint32, c_uint32, _P, _P,
                              POINTER(PprStats)]),

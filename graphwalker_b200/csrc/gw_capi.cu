@@ -1098,4 +1098,35 @@ gw_status gw_probe_gather(gw_ctx* ctx, const uint32_t* d_buf, uint64_t n_words, 
   return GW_OK;
 }
 
+gw_status gw_probe_red(gw_ctx* ctx, uint32_t* d_counters, uint64_t n_words, uint64_t ops, int iters,
+                       double* ops_per_s) {
+  if (!ctx || !d_counters || !ops_per_s || n_words == 0 || ops == 0 || iters < 1)
+    return set_thread_error(GW_E_INVALID, "gw_probe_red: bad argument");
+  uint64_t words = 1;  // counters used: n_words rounded down to a power of two
+  while (words * 2 <= n_words && words < (1ull << 32)) words *= 2;
+  cudaStream_t st = ctx->stream;
+  cudaEvent_t e0, e1;
+  GW_CUDA(ctx, cudaEventCreate(&e0), "event");
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return ctx->fail(GW_E_CUDA, "event");
+  }
+  cudaError_t e = gw::launch_red_probe(d_counters, (uint32_t)(words - 1), ops, st);  // warm-up
+  float best = 1e30f;
+  for (int it = 0; it < iters && e == cudaSuccess; ++it) {
+    cudaEventRecord(e0, st);
+    e = gw::launch_red_probe(d_counters, (uint32_t)(words - 1), ops, st);
+    cudaEventRecord(e1, st);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    best = std::min(best, ms);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return ctx->cuda_fail(e, "red probe");
+  *ops_per_s = (double)ops / (best * 1e-3);
+  return GW_OK;
+}
+
 }  // extern "C"

@@ -119,5 +119,7 @@ cudaError_t launch_partition_scatter(const gw_walk_rec* walks, const uint32_t* d
 // ---- measurement ----
 cudaError_t launch_gather_probe(const uint32_t* buf, uint64_t n_words, uint64_t loads,
                                 unsigned long long* sink, cudaStream_t stream);
+// `ops` red.add of 1 at pseudo-random counters of counters[0 .. mask].
+cudaError_t launch_red_probe(uint32_t* counters, uint32_t mask, uint64_t ops, cudaStream_t stream);
 
 }  // namespace gw

@@ -287,6 +287,22 @@ __global__ void __launch_bounds__(256)
   if (acc == 0x9e3779b9u) atomicAdd(sink, 1ull);
 }
 
+// Random visit-counter updates alone: `ops` red.add of 1 at pseudo-random
+// counters of c[0 .. mask] (mask + 1 a power of two), with the counters'
+// evict_last policy, the same instruction the walk kernels count visits with.
+__global__ void __launch_bounds__(256)
+    red_probe_kernel(uint32_t* __restrict__ c, uint32_t mask, uint64_t ops) {
+  const uint64_t pol = l2_policy(false, true);
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ops; i += stride) {
+    uint32_t h = (uint32_t)i * 0x9E3779B9u + (uint32_t)(i >> 32);
+    h ^= h >> 16;
+    h *= 0x7FEB352Du;
+    h ^= h >> 15;
+    red_add_u32(c + (h & mask), 1u, pol);
+  }
+}
+
 int g_num_sms = 0;
 
 int num_sms() {
@@ -446,6 +462,11 @@ cudaError_t launch_gather_probe(const uint32_t* buf, uint64_t n_words, uint64_t 
                                 unsigned long long* sink, cudaStream_t stream) {
   const int grid = num_sms() * 8;
   gather_probe_kernel<<<grid, 256, 0, stream>>>(buf, n_words, loads, sink);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_red_probe(uint32_t* counters, uint32_t mask, uint64_t ops, cudaStream_t stream) {
+  red_probe_kernel<<<num_sms() * 8, 256, 0, stream>>>(counters, mask, ops);
   return cudaGetLastError();
 }
 

@@ -357,6 +357,12 @@ class Graph:
         check(load().gw_probe_gather(self._h, _ptr(buf), n_words, loads, iters, byref(out)), self._h)
         return out.value
 
+    def probe_red(self, counters, n_words: int, ops: int, iters: int = 5) -> float:
+        """Random visit-counter updates per second (gw_probe_red)."""
+        out = c_double()
+        check(load().gw_probe_red(self._h, _ptr(counters), n_words, ops, iters, byref(out)), self._h)
+        return out.value
+
 
 class Server:
     """A continuous-batching PPR query server on one graph (gw_serve_*)."""

@@ -474,6 +474,12 @@ gw_status gw_inject_fault(uint32_t kind, uint32_t after);
    `loads` dependent-free random 4-byte loads; result in *sectors_per_s.     */
 gw_status gw_probe_gather(gw_ctx *ctx, const uint32_t *d_buf, uint64_t n_words, uint64_t loads,
                           int iters, double *bytes_per_s);
+/* Visit-counter update microbenchmark: `ops` red.add of 1 (the instruction
+   and L2 policy the walk kernels count visits with) at pseudo-random counters
+   of d_counters (n_words uint32, rounded down to a power of two, counters
+   modified); result in *ops_per_s.                                          */
+gw_status gw_probe_red(gw_ctx *ctx, uint32_t *d_counters, uint64_t n_words, uint64_t ops, int iters,
+                       double *ops_per_s);
 
 #ifdef __cplusplus
 }
