@@ -205,8 +205,14 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
   const uint32_t* m_colidx = nullptr;
   if (streaming && ctx->mapped_max_walks) {
     void* mp = nullptr;
-    GW_CUDA(ctx, cudaHostGetDevicePointer(&mp, ctx->h_colidx.p, 0), "mapped colidx");
-    m_colidx = static_cast<const uint32_t*>(mp);
+    const cudaError_t me = cudaHostGetDevicePointer(&mp, ctx->h_colidx.p, 0);
+    if (me == cudaSuccess) {
+      m_colidx = static_cast<const uint32_t*>(mp);
+    } else if (ctx->mapped_max_walks == GW_MAPPED_AUTO) {
+      cudaGetLastError();  // no mapped host memory here: the default copies every block
+    } else {
+      return ctx->cuda_fail(me, "mapped colidx (gw_set_mapped_block_walks)");
+    }
   }
   // the most pending walks at which block q runs in place (0 = never)
   auto mapped_limit = [&](uint32_t q) -> uint64_t {
