@@ -1,4 +1,4 @@
-"""Parity at the benchmark configurations' own sizes.
+"""Parity at the benchmark workloads' own sizes.
 
 The headline workload exactly as bench.py runs it (R-MAT scale 24, edge
 factor 16, 33 blocks, one walk per vertex, L = 10, the jump rule, Philox
@@ -30,7 +30,7 @@ def _blocksize_kb(scale, ef, nblocks):
 
 
 @pytest.fixture(scope="module")
-def config1(cuda_device, oracle):
+def rawwalks24(cuda_device, oracle):
     """The scale-24 graph on the device and, from the C generator, on the host."""
     import graphwalker_b200 as gw
     G = gw.Graph.rmat(SCALE1, EF, seed=1, blocksize_kb=_blocksize_kb(SCALE1, EF, NBLOCKS))
@@ -39,8 +39,8 @@ def config1(cuda_device, oracle):
     G.close()
 
 
-def test_config1_device_graph_equals_c_generator(config1, oracle):
-    G, rp, ci = config1
+def test_rawwalks24_device_graph_equals_c_generator(rawwalks24, oracle):
+    G, rp, ci = rawwalks24
     drp, dci = G.export_csr()
     assert np.array_equal(drp, rp) and np.array_equal(dci, ci)
     assert G.nblocks == 33
@@ -48,8 +48,8 @@ def test_config1_device_graph_equals_c_generator(config1, oracle):
 
 
 @pytest.fixture(scope="module")
-def config1_oracle_counts(config1, oracle):
-    _, rp, ci = config1
+def rawwalks24_oracle_counts(rawwalks24, oracle):
+    _, rp, ci = rawwalks24
     cur = np.arange(len(rp) - 1, dtype=np.uint32)
     r = oracle.run_walks(rp, ci, cur, rule=oracle.RULE_JUMP, L=L1, seed=SEED)
     assert r["status"] == 0
@@ -57,13 +57,13 @@ def config1_oracle_counts(config1, oracle):
 
 
 @pytest.mark.parametrize("layout", [1, 0], ids=["edge_records", "csr"])
-def test_config1_counts_equal_oracle_as_benched(config1, config1_oracle_counts, layout):
+def test_rawwalks24_counts_equal_oracle_as_benched(rawwalks24, rawwalks24_oracle_counts, layout):
     """bench.py's timed step: gw_walk_autotune, then gw_walk_device over all
     16,777,216 resident walk records into u32 counters."""
     import torch
 
     import graphwalker_b200 as gw
-    G, _, _ = config1
+    G, _, _ = rawwalks24
     assert G.set_edge_records(layout) == bool(layout)
     nv = G.nv
     v = torch.arange(nv, dtype=torch.int64, device="cuda")
@@ -77,16 +77,16 @@ def test_config1_counts_equal_oracle_as_benched(config1, config1_oracle_counts, 
         G.walk_device(p, walks, nv, counts=counts)
         G.sync()
         got = counts.cpu().numpy().view(np.uint32)
-        assert np.array_equal(got, config1_oracle_counts)
+        assert np.array_equal(got, rawwalks24_oracle_counts)
 
 
-def test_config1_counts_equal_oracle_through_host_api(config1, config1_oracle_counts):
+def test_rawwalks24_counts_equal_oracle_through_host_api(rawwalks24, rawwalks24_oracle_counts):
     """bench.py's e2e call: gw_run_pools with the reference's 64-bit walk
     words in pinned host memory, per-block pools, counts copied back."""
     import torch
 
     import graphwalker_b200 as gw
-    G, _, _ = config1
+    G, _, _ = rawwalks24
     nv = G.nv
     vv = np.arange(nv, dtype=np.uint64)
     blocks = G.blocks.astype(np.int64)
@@ -96,10 +96,10 @@ def test_config1_counts_equal_oracle_through_host_api(config1, config1_oracle_co
     out = torch.zeros(nv, dtype=torch.int32).pin_memory()
     G.run_pools(gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, L1, seed=SEED), words.data_ptr(), offs.data_ptr(),
                 out.data_ptr())
-    assert np.array_equal(out.numpy().view(np.uint32), config1_oracle_counts)
+    assert np.array_equal(out.numpy().view(np.uint32), rawwalks24_oracle_counts)
 
 
-def test_config1_counts_equal_reference_engine(config1, config1_oracle_counts, oracle, tmp_path):
+def test_rawwalks24_counts_equal_reference_engine(rawwalks24, rawwalks24_oracle_counts, oracle, tmp_path):
     """The reference's own engine (graphwalker.hpp), walk manager and
     RandomWalkwithJump, compiled from its sources with rand_r routed to the
     Philox stream, on the scale-24 graph files: the oracle's counts, hence
@@ -108,7 +108,7 @@ def test_config1_counts_equal_reference_engine(config1, config1_oracle_counts, o
     if not exe.exists():
         pytest.skip("the shimmed reference engine is built where the reference tree exists")
     from graphwalker_b200 import formats
-    _, rp, ci = config1
+    _, rp, ci = rawwalks24
     nv = len(rp) - 1
     kb = _blocksize_kb(SCALE1, EF, NBLOCKS)
     base = str(tmp_path / "rmat24")
@@ -129,16 +129,16 @@ def test_config1_counts_equal_reference_engine(config1, config1_oracle_counts, o
     raw = of.read_bytes()
     status, nv_ref = struct.unpack_from("<II", raw, 0)
     assert status == 0 and nv_ref == nv
-    assert np.array_equal(np.frombuffer(raw, np.uint32, nv, 8), config1_oracle_counts)
+    assert np.array_equal(np.frombuffer(raw, np.uint32, nv, 8), rawwalks24_oracle_counts)
 
 
-def test_config1_streamed_blocks_equal_oracle(config1, config1_oracle_counts):
-    """Config 3's path at config 1's size: the CSR held in pinned host memory,
+def test_rawwalks24_streamed_blocks_equal_oracle(rawwalks24, rawwalks24_oracle_counts):
+    """The out-of-core path at the scale-24 raw-walk size: the CSR held in pinned host memory,
     8 device block slots for 33 blocks, the blocked engine (state-aware block
     choice, block copies on a side stream, eviction of the block with the
     fewest walks).  Counts equal the oracle's."""
     import graphwalker_b200 as gw
-    G, _, _ = config1
+    G, _, _ = rawwalks24
     try:
         G.walks_clear()
         G.add_walks_at(np.arange(G.nv, dtype=np.uint32))
@@ -150,7 +150,7 @@ def test_config1_streamed_blocks_equal_oracle(config1, config1_oracle_counts):
             G.set_mapped_block_walks(limit)
             st = G.run(gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, L1, seed=SEED, mode=gw.MODE_BLOCKED,
                                  prob=0.2))
-            assert np.array_equal(G.read_counts(), config1_oracle_counts), limit
+            assert np.array_equal(G.read_counts(), rawwalks24_oracle_counts), limit
             steps = steps or st.supersteps
             assert st.supersteps == steps  # the same block order
             if limit == 0:
@@ -162,9 +162,9 @@ def test_config1_streamed_blocks_equal_oracle(config1, config1_oracle_counts):
         G.set_residency(gw.RESIDENT_HBM)
 
 
-# ---------------------------------------------------------------- config 0
+# ---------------------------------------------------------------- single-source PPR, scale 20
 @pytest.fixture(scope="module")
-def config0(cuda_device, oracle):
+def ppr20(cuda_device, oracle):
     import graphwalker_b200 as gw
     G = gw.Graph.rmat(20, EF, seed=1, blocksize_kb=_blocksize_kb(20, EF, 16))
     rp, ci = G.export_csr()
@@ -180,7 +180,7 @@ def _source_walks(src, B, first_id=0):
     return w.to(torch.int32).contiguous()
 
 
-def test_config0_counts_and_top100_equal_oracle(config0, oracle):
+def test_ppr20_counts_and_top100_equal_oracle(ppr20, oracle):
     """100,000 walks from the top vertex under the PPR rule (stop w.p. 0.15,
     a dangling vertex returns the walk to its source, at most 20 hops): the
     counts of the device walk launch and the top-100 of gw_ppr_run equal the
@@ -189,7 +189,7 @@ def test_config0_counts_and_top100_equal_oracle(config0, oracle):
 
     import graphwalker_b200 as gw
     from graphwalker_b200 import accuracy
-    G, rp, ci, src = config0
+    G, rp, ci, src = ppr20
     B, L = 100_000, 20
     ref = oracle.run_walks(rp, ci, np.full(B, src, np.uint32), ids=np.arange(B, dtype=np.uint32),
                            src=np.full(B, src, np.uint32), rule=oracle.RULE_PPR, L=L, seed=SEED)
@@ -210,7 +210,7 @@ def test_config0_counts_and_top100_equal_oracle(config0, oracle):
 
 
 @pytest.mark.parametrize("rule", [4, 1], ids=["ppr", "stop"])
-def test_config0_accuracy_within_monte_carlo_noise(config0, rule):
+def test_ppr20_accuracy_within_monte_carlo_noise(ppr20, rule):
     """The estimate's L1 error and top-100 overlap against the FP64 power
     series lie within three standard deviations of what Poisson noise at
     this budget predicts, over several seeds."""
@@ -218,7 +218,7 @@ def test_config0_accuracy_within_monte_carlo_noise(config0, rule):
 
     import graphwalker_b200 as gw
     from graphwalker_b200 import accuracy
-    G, _, _, src = config0
+    G, _, _, src = ppr20
     B, L = 100_000, 20
     mu = G.expected_visits(gw.params(rule, gw.SINK_NONE, L), src)
     assert mu[src] >= 1.0
@@ -240,8 +240,8 @@ def test_config0_accuracy_within_monte_carlo_noise(config0, rule):
     assert exp["expected_l1"] <= exp["l1_bound"]
 
 
-# ---------------------------------------------------------------- config 2
-def test_config2_subset_top100_equals_oracle(cuda_device, oracle):
+# ---------------------------------------------------------------- multi-source PPR, scale 26
+def test_msppr26_subset_top100_equals_oracle(cuda_device, oracle):
     """The scale-26 msppr batch as benched (4,096 queries, sources uniform
     over out-degree >= 1, budgets round(10^U(2,5)), stop rule, L <= 20,
     top-100), batched in one launch; 64 of its queries (every 64th, with
