@@ -558,7 +558,15 @@ cudaError_t query_dispatch(const QueryView& qv, unsigned long long w_begin, unsi
   const unsigned long long need = (n + kPprThreads - 1) / kPprThreads;
   const unsigned long long full = (unsigned long long)sms * per_sm;
   const int grid = (int)(need < full ? (need ? need : 1) : full);
-  kern<<<grid, kPprThreads, 0, stream>>>(qv, w_begin, w_end, g, a, status);
+  // Walks per cursor grab: no larger than gives every warp of the grid a
+  // share, so a launch of few walks (one query, a small serving step) runs
+  // them side by side instead of a lane's worth of walks one after another.
+  QueryView q = qv;
+  const unsigned long long warps = (unsigned long long)grid * (kPprThreads / 32);
+  const unsigned long long fair = ((n + warps - 1) / warps + 31) / 32 * 32;
+  const unsigned long long chunk = qv.chunk ? qv.chunk : kWarpChunk;
+  q.chunk = (uint32_t)(fair < chunk ? fair : chunk);
+  kern<<<grid, kPprThreads, 0, stream>>>(q, w_begin, w_end, g, a, status);
   return cudaGetLastError();
 }
 
