@@ -87,7 +87,11 @@ gw_status plan_set(gw_ctx* ctx, const uint32_t* sources, const uint32_t* budgets
   return GW_OK;
 }
 
-gw_status upload_set(gw_ctx* ctx, QuerySet* s, uint32_t k, cudaStream_t st) {
+// batched: the top-k segments grow with the set (64 queries per doubling),
+// so one launch ranks the whole set; one query at a time (plain), every table
+// splits into kTopkSegment-slot segments, so a large table is ranked by many
+// CTAs instead of one.
+gw_status upload_set(gw_ctx* ctx, QuerySet* s, uint32_t k, cudaStream_t st, bool batched) {
   const uint32_t n = (uint32_t)s->qmap.size();
   GW_CUDA(ctx, s->d_sources->ensure(n * 4), "query alloc");
   GW_CUDA(ctx, s->d_prefix->ensure((n + 1) * 8), "query alloc");
@@ -103,7 +107,7 @@ gw_status upload_set(gw_ctx* ctx, QuerySet* s, uint32_t k, cudaStream_t st) {
   GW_CUDA(ctx, s->d_cnt->ensure((uint64_t)n * k * 4), "top-k alloc");
   GW_CUDA(ctx, s->d_cursor->ensure(sizeof(unsigned long long)), "query alloc");
   s->seg_first.resize(n + 1);
-  s->seg_slots = gw::topk_segment_slots(n);
+  s->seg_slots = batched ? gw::topk_segment_slots(n) : gw::kTopkSegment;
   gw::topk_segment_prefix(s->tmask.data(), n, s->seg_slots, s->seg_first.data());
   s->seg_order.resize(s->seg_first[n]);
   gw::topk_segment_order(s->tmask.data(), n, s->seg_slots, s->seg_first.data(), s->seg_order.data());
@@ -246,11 +250,11 @@ extern "C" gw_status gw_ppr_run(gw_ctx* ctx, const gw_walk_params* params, const
   for (int round = 0; round <= kMaxRetries && !which.empty(); ++round) {
     QuerySet set(ctx, round == 0);
     s = plan_set(ctx, sources, budgets, ids.data(), which, factor, &set);
-    if (s == GW_OK) s = upload_set(ctx, &set, k, st);
+    const bool b = batched || round > 0;
+    if (s == GW_OK) s = upload_set(ctx, &set, k, st, b);
     if (s != GW_OK) break;
     set.qv.visits = ctx->d_q_visits.as<unsigned long long>();
     set.qv.chunk = ctx->ppr_chunk;
-    const bool b = batched || round > 0;
     cudaError_t e = run_set(ctx, params, a, &set, k, b, b ? ctx->ppr_threads_per_sm : 0, st, ev, &local.launches);
     const uint32_t n = (uint32_t)which.size();
     // The first round holds every query in the caller's order: its lists go
@@ -332,7 +336,7 @@ extern "C" gw_status gw_ppr_autotune(gw_ctx* ctx, const gw_walk_params* params, 
   for (uint32_t q = 0; q < nq; ++q) which[q] = q;
   QuerySet set(ctx, true);
   s = plan_set(ctx, sources, budgets, ids.data(), which, params->table_factor ? params->table_factor : 8, &set);
-  if (s == GW_OK) s = upload_set(ctx, &set, 1, ctx->stream);
+  if (s == GW_OK) s = upload_set(ctx, &set, 1, ctx->stream, true);
   if (s != GW_OK) return s;
   cudaStream_t st = ctx->stream;
   cudaEvent_t e0, e1;
