@@ -81,7 +81,7 @@ class RunStats(Structure):
     _fields_ = [("walks", c_uint64), ("supersteps", c_uint64), ("block_loads", c_uint64),
                 ("bytes_h2d", c_uint64), ("ms_total", c_double), ("ms_walk", c_double),
                 ("ms_partition", c_double), ("ms_copy_wait", c_double), ("mapped_supersteps", c_uint64),
-                ("mapped_walks", c_uint64)]
+                ("mapped_walks", c_uint64), ("pools_spilled", c_uint64), ("pools_refilled", c_uint64)]
 
 
 class GraphDesc(Structure):
@@ -118,6 +118,7 @@ _SIGS = {
     "gw_export_csr": (c_int32, [_P, _P, _P]),
     "gw_set_residency": (c_int32, [_P, c_uint32, c_uint32]),
     "gw_set_mapped_block_walks": (c_int32, [_P, c_uint64]),
+    "gw_set_pool_budget": (c_int32, [_P, c_uint64]),
     "gw_walks_clear": (c_int32, [_P]),
     "gw_walks_add": (c_int32, [_P, c_uint32, _P, _P, c_size_t]),
     "gw_walks_count": (c_int32, [_P, _P, POINTER(c_uint64)]),

@@ -556,6 +556,12 @@ gw_status gw_set_residency(gw_ctx* ctx, uint32_t residency, uint32_t nmblocks) {
   return apply_edge_records(ctx);
 }
 
+gw_status gw_set_pool_budget(gw_ctx* ctx, uint64_t bytes) {
+  if (!ctx) return set_thread_error(GW_E_INVALID, "NULL context");
+  ctx->pool_budget = bytes;
+  return GW_OK;
+}
+
 gw_status gw_set_mapped_block_walks(gw_ctx* ctx, uint64_t max_walks) {
   if (!ctx) return set_thread_error(GW_E_INVALID, "NULL context");
   ctx->mapped_max_walks = max_walks;
@@ -834,8 +840,13 @@ gw_status gw_read_pool(gw_ctx* ctx, uint32_t block, gw_walk_rec* out, size_t cap
   const uint64_t size = block < ctx->pool_size.size() ? ctx->pool_size[block] : 0;
   *n = size;
   const uint64_t m = std::min<uint64_t>(size, cap);
-  if (m && out)
-    GW_CUDA(ctx, cudaMemcpy(out, ctx->pools[block].p, m * sizeof(gw_walk_rec), cudaMemcpyDeviceToHost),
+  if (!m || !out) return GW_OK;
+  // the part moved to host memory comes first (older walks), then the device part
+  const std::vector<gw_walk_rec>* host = block < ctx->pool_host.size() ? &ctx->pool_host[block] : nullptr;
+  const uint64_t hn = host ? std::min<uint64_t>(host->size(), m) : 0;
+  if (hn) std::copy(host->begin(), host->begin() + hn, out);
+  if (m > hn)
+    GW_CUDA(ctx, cudaMemcpy(out + hn, ctx->pools[block].p, (m - hn) * sizeof(gw_walk_rec), cudaMemcpyDeviceToHost),
             "pool read");
   return GW_OK;
 }

@@ -113,6 +113,12 @@ struct gw_ctx {
   gw_devbuf d_dest, d_tile_hist, d_tile_off, d_totals, d_minhop, d_scan_temp, d_out_ptr,
       d_out_base;
   std::vector<gw_devbuf> pools;   // per-block device pools
+  // The older part of each block's pool, moved to host memory when the device
+  // pools exceed pool_budget bytes (0 = no limit).  A block's pool is this
+  // part followed by the first pool_size - pool_host.size() records on the
+  // device.
+  std::vector<std::vector<gw_walk_rec>> pool_host;
+  uint64_t pool_budget = 0;
   std::vector<uint64_t> pool_size;
   std::vector<uint32_t> minstep;  // per-block min hop (WalkManager::minstep)
 

@@ -117,10 +117,57 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
 
   // ---- initial pools (startWalks; getCurrentWalks reads them back) ----
   ctx->pools.resize(nb);
+  ctx->pool_host.assign(nb, {});
   ctx->pool_size.assign(nb, 0);
   ctx->minstep.assign(nb, 0xffff);
+  ctx->stats = gw_run_stats{};
   std::vector<uint64_t> cap(nb, 0);
   for (uint32_t b = 0; b < nb; ++b) cap[b] = ctx->pools[b].bytes / sizeof(gw_walk_rec);
+  // Grown pools come from the stream-ordered allocator, so replacing one
+  // queues its free behind the copy out of it; a pool from gw_walks_add is
+  // retired instead and freed with the events.
+  std::vector<char> pool_async(nb, 0);
+  // records of block d's pool held on the device (after its host part)
+  auto dev_n = [&](uint32_t d) { return ctx->pool_size[d] - ctx->pool_host[d].size(); };
+  // writeWalks2Disk: while the device pools hold more than the budget, the
+  // pools with the fewest pending walks (never the fullest) move to host
+  // memory, empty pools first giving back their room.
+  auto spill_to_budget = [&]() -> cudaError_t {
+    if (!ctx->pool_budget) return cudaSuccess;
+    uint64_t held = 0;
+    for (uint32_t d = 0; d < nb; ++d) held += cap[d];
+    if (held * sizeof(gw_walk_rec) <= ctx->pool_budget) return cudaSuccess;
+    cudaError_t e = cudaStreamSynchronize(st);  // queued scatters into the pools are done
+    uint32_t fullest = 0;
+    for (uint32_t d = 1; d < nb; ++d)
+      if (ctx->pool_size[d] > ctx->pool_size[fullest]) fullest = d;
+    std::vector<uint32_t> order;
+    for (uint32_t d = 0; d < nb; ++d)
+      if (cap[d] && d != fullest) order.push_back(d);
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+      const bool ex = dev_n(x) == 0, ey = dev_n(y) == 0;
+      return ex != ey ? ex : ctx->pool_size[x] < ctx->pool_size[y];
+    });
+    for (size_t i = 0; i < order.size() && e == cudaSuccess && held * sizeof(gw_walk_rec) > ctx->pool_budget; ++i) {
+      const uint32_t d = order[i];
+      const uint64_t dn = dev_n(d);
+      if (dn) {
+        std::vector<gw_walk_rec>& h = ctx->pool_host[d];
+        const size_t old = h.size();
+        h.resize(old + dn);
+        e = cudaMemcpy(h.data() + old, ctx->pools[d].p, dn * sizeof(gw_walk_rec), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) break;
+        ctx->stats.pools_spilled++;
+      }
+      e = pool_async[d] ? cudaFreeAsync(ctx->pools[d].p, st) : cudaFree(ctx->pools[d].p);
+      ctx->pools[d].p = nullptr;
+      ctx->pools[d].bytes = 0;
+      held -= cap[d];
+      cap[d] = 0;
+      pool_async[d] = 0;
+    }
+    return e;
+  };
   uint64_t walksum = 0, maxpool = 0;
   for (uint32_t b = 0; b < nb; ++b) maxpool = std::max<uint64_t>(maxpool, ctx->pool_words[b].size());
   GW_CUDA(ctx, ctx->d_words.ensure(maxpool * 8), "word alloc");
@@ -144,6 +191,7 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     ctx->pool_size[b] = m;
     for (uint64_t w : ctx->pool_words[b]) ctx->minstep[b] = std::min<uint32_t>(ctx->minstep[b], gw_get_hop(w));
     walksum += m;
+    GW_CUDA(ctx, spill_to_budget(), "pool spill");
   }
   const uint64_t nwalks = walksum;
   walksum = 0;  // from here on: walks pending in the owned blocks
@@ -221,7 +269,6 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     const uint64_t* hr = ctx->h_rowptr.as<uint64_t>();
     return (hr[ctx->blocks[q + 1]] - hr[ctx->blocks[q]]) * 4 / kMappedBytesPerWalk;
   };
-  ctx->stats = gw_run_stats{};
   ctx->stats.walks = nwalks;
 
   std::vector<uint32_t> ahead;  // blocks copied ahead of their turn, not yet run
@@ -288,10 +335,6 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     ms_walk += w;
     ms_partition += m;
   };
-  // Grown pools come from the stream-ordered allocator, so replacing one
-  // queues its free behind the copy out of it; a pool from gw_walks_add is
-  // retired instead and freed with the events.
-  std::vector<char> pool_async(nb, 0);
   cudaEventRecord(t0, st);
   uint64_t superstep = 0;
   cudaError_t e = cudaSuccess;
@@ -315,6 +358,33 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     const uint64_t n = ctx->pool_size[b];
     if (n == 0) return ctx->fail(GW_E_STATE, "scheduler chose an empty block (walksum %llu)",
                                  (unsigned long long)walksum);
+    if (!ctx->pool_host[b].empty()) {
+      // readWalksfromDisk: the pool's host part (its older walks) goes first,
+      // then the walks that arrived on the device since it moved out
+      const uint64_t hn = ctx->pool_host[b].size(), dn = n - hn;
+      const uint64_t ncap = std::max<uint64_t>(n, 1024);
+      void* np = nullptr;
+      e = cudaMallocAsync(&np, ncap * sizeof(gw_walk_rec), st);
+      if (e != cudaSuccess) break;
+      // from pageable memory: the records are staged before the call returns
+      e = cudaMemcpyAsync(np, ctx->pool_host[b].data(), hn * sizeof(gw_walk_rec), cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess && dn)
+        e = cudaMemcpyAsync(static_cast<gw_walk_rec*>(np) + hn, ctx->pools[b].p, dn * sizeof(gw_walk_rec),
+                            cudaMemcpyDeviceToDevice, st);
+      if (ctx->pools[b].p) {
+        if (pool_async[b])
+          cudaFreeAsync(ctx->pools[b].p, st);
+        else
+          evs.retired.push_back(ctx->pools[b].p);
+      }
+      pool_async[b] = 1;
+      ctx->pools[b].p = np;
+      ctx->pools[b].bytes = ncap * sizeof(gw_walk_rec);
+      cap[b] = ncap;
+      std::vector<gw_walk_rec>().swap(ctx->pool_host[b]);
+      ctx->stats.pools_refilled++;
+      if (e != cudaSuccess) break;
+    }
     WalkArgs ab = a;
     ab.lo = ctx->blocks[b];
     ab.hi = ctx->blocks[b + 1];
@@ -395,16 +465,16 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     if (superstep > 0) add_phases(superstep - 1);
     // updateWalkNum: grow destination pools, then scatter into them
     for (uint32_t d = 0; d < nb; ++d) {
-      const uint64_t need = ctx->pool_size[d] + h_totals[d];
+      const uint64_t held = dev_n(d);  // the device part; a host part stays where it is
+      const uint64_t need = held + h_totals[d];
       if (d != b && need > cap[d]) {
         uint64_t ncap = std::max<uint64_t>(need, cap[d] * 2);
         ncap = std::max<uint64_t>(ncap, 1024);
         void* np = nullptr;
         e = cudaMallocAsync(&np, ncap * sizeof(gw_walk_rec), st);
         if (e != cudaSuccess) break;
-        if (ctx->pool_size[d])
-          e = cudaMemcpyAsync(np, ctx->pools[d].p, ctx->pool_size[d] * sizeof(gw_walk_rec),
-                              cudaMemcpyDeviceToDevice, st);
+        if (held)
+          e = cudaMemcpyAsync(np, ctx->pools[d].p, held * sizeof(gw_walk_rec), cudaMemcpyDeviceToDevice, st);
         if (ctx->pools[d].p) {
           if (pool_async[d])
             cudaFreeAsync(ctx->pools[d].p, st);
@@ -418,7 +488,7 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
         if (e != cudaSuccess) break;
       }
       h_ptr[d] = ctx->pools[d].as<gw_walk_rec>();
-      h_base[d] = ctx->pool_size[d];
+      h_base[d] = dev_n(d);
     }
     if (e != cudaSuccess) break;
     h_ptr[nb] = nullptr;
@@ -446,6 +516,7 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     ctx->pool_size[b] = 0;
     ctx->minstep[b] = 0xffff;
     ++superstep;
+    e = spill_to_budget();
   }
   cudaEventRecord(t1, st);
   if (e != cudaSuccess) return ctx->cuda_fail(e, "blocked engine");

@@ -173,6 +173,11 @@ class Graph:
         """Moves the CSR between HBM and pinned host memory (streamed blocks)."""
         check(load().gw_set_residency(self._h, residency, nmblocks), self._h)
 
+    def set_pool_budget(self, nbytes: int) -> None:
+        """Device bytes the blocked engine's walk pools may hold (0 = no limit);
+        past it, pools move to host memory and come back when their block runs."""
+        check(load().gw_set_pool_budget(self._h, nbytes), self._h)
+
     def set_mapped_block_walks(self, max_walks: int) -> None:
         """Streamed blocks with at most max_walks pending walks (and in no
         device slot) are read in place from pinned host memory, not copied."""

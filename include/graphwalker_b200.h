@@ -137,6 +137,8 @@ typedef struct gw_run_stats {
   uint64_t mapped_supersteps; /* block executions read in place from pinned
                                  host memory (streaming, gw_set_mapped_block_walks) */
   uint64_t mapped_walks;   /* walks those executions advanced                 */
+  uint64_t pools_spilled;  /* block pools moved to host memory (pool budget)  */
+  uint64_t pools_refilled; /* spilled pools brought back to run their block   */
 } gw_run_stats;
 
 /* ---- version / codec (host only, no device needed) -------------------- */
@@ -202,6 +204,15 @@ gw_status gw_set_residency(gw_ctx *ctx, uint32_t residency, uint32_t nmblocks);
    128 bytes of its column slice.                                            */
 #define GW_MAPPED_AUTO 0xFFFFFFFFFFFFFFFFull
 gw_status gw_set_mapped_block_walks(gw_ctx *ctx, uint64_t max_walks);
+/* Device bytes the blocked engine's walk pools may hold (0, the default: no
+   limit).  Past it, after a superstep, whole pools move to host memory, the
+   pools with the fewest pending walks first (never the fullest, the likely
+   next choice), as WalkManager::writeWalks2Disk spills pool buffers
+   (walk.hpp:103-112); a block whose pool was moved is brought back, older
+   walks first, when it is chosen (readWalksfromDisk, walk.hpp:139-157).  Pool
+   order, walks and counts are unchanged; the pool of the block being run may
+   exceed the budget.  This lets the walk state outgrow the device.          */
+gw_status gw_set_pool_budget(gw_ctx *ctx, uint64_t bytes);
 
 /* ---- walk pools (WalkManager) ------------------------------------------- */
 gw_status gw_walks_clear(gw_ctx *ctx);

@@ -195,6 +195,34 @@ def test_blocked_pools_are_stable_partitions(cuda_device, oracle, steps):
             assert np.array_equal(pool, exp), f"block {b}"
 
 
+@pytest.mark.parametrize("steps", [3, 7, 0])
+@pytest.mark.parametrize("residency", [0, 1], ids=["hbm", "streamed"])
+def test_pool_budget_spills_pools_in_order(cuda_device, oracle, steps, residency):
+    """A device budget far below the walk state: pools move to host memory and
+    come back when their block runs.  Pools after k supersteps (their host part
+    first) still equal the stable-pool restatement, and the full run's counts
+    and superstep count equal the reference loop's."""
+    import graphwalker_b200 as gw
+    g = load_golden("rmat13")
+    cur = g["jump_cur"]
+    ref = oracle.block_engine(g["rowptr"], g["colidx"], g["blocks"], cur, rule=0, L=10,
+                              seed=int(g["seed"]), prob=0.2, max_supersteps=steps)
+    with _graph(g, residency) as G:
+        G.set_pool_budget(48 * 1024)  # 3072 walk records; the run holds 8192 walks
+        _add_golden_walks(G, g, "jump")
+        st = G.run(gw.params(0, gw.SINK_VERTEX_COUNT, 10, seed=int(g["seed"]), mode=gw.MODE_BLOCKED,
+                             prob=0.2, max_supersteps=steps))
+        assert st.supersteps == ref["supersteps"]
+        assert np.array_equal(G.read_counts(), ref["counts"])
+        assert st.pools_spilled > 0 and st.pools_refilled > 0
+        for b in range(G.nblocks):
+            pool = G.read_pool(b)
+            exp = np.stack(ref["pools"][b], axis=1) if len(ref["pools"][b][0]) else np.zeros((0, 4), np.uint32)
+            assert np.array_equal(pool, exp), f"block {b}"
+        if steps == 0:
+            assert np.array_equal(G.read_counts(), g["jump_counts"])
+
+
 def test_device_rmat_matches_oracle(cuda_device, oracle):
     import graphwalker_b200 as gw
     for scale, ef, seed in [(10, 16, 1), (13, 8, 3), (16, 16, 9)]:
