@@ -96,6 +96,9 @@ def parse_args():
                     help="gather: the buffer in pinned host memory, read by the kernel over the host link")
     ap.add_argument("--sink", choices=["count", "none"], default="count",
                     help="walkonly: count visits per vertex (the headline's sink) or record nothing")
+    ap.add_argument("--pool-budget-mb", type=int, default=0,
+                    help="ooc: also run the streamed block loop with its walk pools held to this many MB of device "
+                         "memory (gw_set_pool_budget), the rest spilled to host memory")
     ap.add_argument("--mapped-walks", default="auto",
                     help="ooc: gw_set_mapped_block_walks of the default streamed run ('auto' or a number)")
     ap.add_argument("--rng", choices=["philox", "native"], default="philox", help="walkonly: random stream")
@@ -991,14 +994,18 @@ def ooc_measure(args) -> dict:
         t_first = time.perf_counter()
         G.run(gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, L, seed=args.walk_seed, mode=gw.MODE_BLOCKED, prob=0.2))
         first_s = time.perf_counter() - t_first
-        for name, residency, mode, mapped in (
-                ("resident_one_launch", gw.RESIDENT_HBM, gw.MODE_RESIDENT, gw.MAPPED_AUTO),
-                ("resident_blocked", gw.RESIDENT_HBM, gw.MODE_BLOCKED, gw.MAPPED_AUTO),
-                ("streamed_blocked_copy_all", gw.STREAM_PINNED, gw.MODE_BLOCKED, 0),
-                ("streamed_blocked", gw.STREAM_PINNED, gw.MODE_BLOCKED,
-                 gw.MAPPED_AUTO if args.mapped_walks == "auto" else int(args.mapped_walks))):
+        mapped_default = gw.MAPPED_AUTO if args.mapped_walks == "auto" else int(args.mapped_walks)
+        modes = [("resident_one_launch", gw.RESIDENT_HBM, gw.MODE_RESIDENT, gw.MAPPED_AUTO, 0),
+                 ("resident_blocked", gw.RESIDENT_HBM, gw.MODE_BLOCKED, gw.MAPPED_AUTO, 0),
+                 ("streamed_blocked_copy_all", gw.STREAM_PINNED, gw.MODE_BLOCKED, 0, 0),
+                 ("streamed_blocked", gw.STREAM_PINNED, gw.MODE_BLOCKED, mapped_default, 0)]
+        if args.pool_budget_mb:
+            modes.append(("streamed_blocked_pool_budget", gw.STREAM_PINNED, gw.MODE_BLOCKED, mapped_default,
+                          args.pool_budget_mb << 20))
+        for name, residency, mode, mapped, budget in modes:
             G.set_residency(residency, nmblocks=slots)
             G.set_mapped_block_walks(mapped)
+            G.set_pool_budget(budget)
             st = G.run(gw.params(gw.RULE_JUMP, gw.SINK_VERTEX_COUNT, L, seed=args.walk_seed, mode=mode, prob=0.2))
             counts = G.read_counts()
             if int(counts.astype(np.int64).sum()) != nv * L:
@@ -1013,6 +1020,8 @@ def ooc_measure(args) -> dict:
                          "h2d_GBps": st.bytes_h2d / (st.ms_total * 1e-3) / 1e9 if st.bytes_h2d else 0.0,
                          "blocks_read_in_place": {"supersteps": int(st.mapped_supersteps),
                                                   "walks": int(st.mapped_walks)},
+                         "pools": {"budget_bytes": int(budget), "spilled": int(st.pools_spilled),
+                                   "refilled": int(st.pools_refilled)},
                          "device_ms": {"walk": st.ms_walk, "partition": st.ms_partition,
                                        "copy_wait": st.ms_copy_wait}}
         link = host_link_gbps()

@@ -487,6 +487,7 @@ gw_status gw_close(gw_ctx* ctx) {
   ctx->h_rowptr.release();
   ctx->h_colidx.release();
   ctx->h_status.release();
+  ctx->pool_arena.release();
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   if (ctx->aux_stream) cudaStreamDestroy(ctx->aux_stream);
@@ -842,9 +843,15 @@ gw_status gw_read_pool(gw_ctx* ctx, uint32_t block, gw_walk_rec* out, size_t cap
   const uint64_t m = std::min<uint64_t>(size, cap);
   if (!m || !out) return GW_OK;
   // the part moved to host memory comes first (older walks), then the device part
-  const std::vector<gw_walk_rec>* host = block < ctx->pool_host.size() ? &ctx->pool_host[block] : nullptr;
-  const uint64_t hn = host ? std::min<uint64_t>(host->size(), m) : 0;
-  if (hn) std::copy(host->begin(), host->begin() + hn, out);
+  const uint64_t hn = block < ctx->pool_host_n.size() ? std::min<uint64_t>(ctx->pool_host_n[block], m) : 0;
+  if (hn) {
+    GW_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "pool read");
+    const gw_walk_rec* arena = ctx->pool_arena.as<gw_walk_rec>();
+    for (uint64_t i = 0; i * gw_ctx::kPoolChunk < hn; ++i) {
+      const uint64_t c = ctx->pool_chunks[block][i], k = std::min(gw_ctx::kPoolChunk, hn - i * gw_ctx::kPoolChunk);
+      std::copy(arena + c * gw_ctx::kPoolChunk, arena + c * gw_ctx::kPoolChunk + k, out + i * gw_ctx::kPoolChunk);
+    }
+  }
   if (m > hn)
     GW_CUDA(ctx, cudaMemcpy(out + hn, ctx->pools[block].p, (m - hn) * sizeof(gw_walk_rec), cudaMemcpyDeviceToHost),
             "pool read");

@@ -114,10 +114,15 @@ struct gw_ctx {
       d_out_base;
   std::vector<gw_devbuf> pools;   // per-block device pools
   // The older part of each block's pool, moved to host memory when the device
-  // pools exceed pool_budget bytes (0 = no limit).  A block's pool is this
-  // part followed by the first pool_size - pool_host.size() records on the
+  // pools exceed pool_budget bytes (0 = no limit): pool_host_n[b] records in
+  // the pinned arena's chunks pool_chunks[b], in order.  A block's pool is
+  // this part followed by the first pool_size - pool_host_n records on the
   // device.
-  std::vector<std::vector<gw_walk_rec>> pool_host;
+  static constexpr uint64_t kPoolChunk = 65536;  // walk records per arena chunk (1 MiB)
+  gw_hostbuf pool_arena;
+  std::vector<uint32_t> arena_free;               // chunks not in use
+  std::vector<std::vector<uint32_t>> pool_chunks;
+  std::vector<uint64_t> pool_host_n;
   uint64_t pool_budget = 0;
   std::vector<uint64_t> pool_size;
   std::vector<uint32_t> minstep;  // per-block min hop (WalkManager::minstep)

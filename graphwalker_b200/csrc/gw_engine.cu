@@ -117,7 +117,8 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
 
   // ---- initial pools (startWalks; getCurrentWalks reads them back) ----
   ctx->pools.resize(nb);
-  ctx->pool_host.assign(nb, {});
+  ctx->pool_chunks.assign(nb, {});
+  ctx->pool_host_n.assign(nb, 0);
   ctx->pool_size.assign(nb, 0);
   ctx->minstep.assign(nb, 0xffff);
   ctx->stats = gw_run_stats{};
@@ -128,16 +129,29 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
   // retired instead and freed with the events.
   std::vector<char> pool_async(nb, 0);
   // records of block d's pool held on the device (after its host part)
-  auto dev_n = [&](uint32_t d) { return ctx->pool_size[d] - ctx->pool_host[d].size(); };
-  // writeWalks2Disk: while the device pools hold more than the budget, the
+  auto dev_n = [&](uint32_t d) { return ctx->pool_size[d] - ctx->pool_host_n[d]; };
+  constexpr uint64_t kChunk = gw_ctx::kPoolChunk;
+  if (ctx->pool_budget) {
+    // pinned chunks for every walk of the run, plus a partly filled one per block
+    uint64_t total = 0;
+    for (uint32_t b = 0; b < nb; ++b) total += ctx->pool_words[b].size();
+    const uint64_t nchunks = (total + kChunk - 1) / kChunk + nb;
+    GW_CUDA(ctx, ctx->pool_arena.ensure(nchunks * kChunk * sizeof(gw_walk_rec)), "pool arena");
+    ctx->arena_free.resize(nchunks);
+    for (uint64_t c = 0; c < nchunks; ++c) ctx->arena_free[c] = (uint32_t)(nchunks - 1 - c);
+  }
+  gw_walk_rec* const arena = ctx->pool_arena.as<gw_walk_rec>();
+  // writeWalks2Disk: once the device pools hold more than the budget, the
   // pools with the fewest pending walks (never the fullest) move to host
-  // memory, empty pools first giving back their room.
+  // memory, empty pools first giving back their room, until they hold half
+  // of it: the headroom takes many supersteps' arrivals before the next
+  // spill, so pools move out in a few large batches, not a few every step.
   auto spill_to_budget = [&]() -> cudaError_t {
     if (!ctx->pool_budget) return cudaSuccess;
     uint64_t held = 0;
     for (uint32_t d = 0; d < nb; ++d) held += cap[d];
     if (held * sizeof(gw_walk_rec) <= ctx->pool_budget) return cudaSuccess;
-    cudaError_t e = cudaStreamSynchronize(st);  // queued scatters into the pools are done
+    const uint64_t low = ctx->pool_budget / 2;
     uint32_t fullest = 0;
     for (uint32_t d = 1; d < nb; ++d)
       if (ctx->pool_size[d] > ctx->pool_size[fullest]) fullest = d;
@@ -148,23 +162,42 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
       const bool ex = dev_n(x) == 0, ey = dev_n(y) == 0;
       return ex != ey ? ex : ctx->pool_size[x] < ctx->pool_size[y];
     });
-    for (size_t i = 0; i < order.size() && e == cudaSuccess && held * sizeof(gw_walk_rec) > ctx->pool_budget; ++i) {
+    // Copies out and frees of stream-ordered pools queue on st behind the
+    // scatter that filled them; pools from gw_walks_add are freed after a
+    // synchronisation.
+    cudaError_t e = cudaSuccess;
+    std::vector<void*> sync_free;
+    for (size_t i = 0; i < order.size() && e == cudaSuccess && held * sizeof(gw_walk_rec) > low; ++i) {
       const uint32_t d = order[i];
       const uint64_t dn = dev_n(d);
-      if (dn) {
-        std::vector<gw_walk_rec>& h = ctx->pool_host[d];
-        const size_t old = h.size();
-        h.resize(old + dn);
-        e = cudaMemcpy(h.data() + old, ctx->pools[d].p, dn * sizeof(gw_walk_rec), cudaMemcpyDeviceToHost);
-        if (e != cudaSuccess) break;
-        ctx->stats.pools_spilled++;
+      for (uint64_t off = 0; off < dn && e == cudaSuccess;) {
+        uint64_t& hn = ctx->pool_host_n[d];
+        const uint64_t used = hn % kChunk;
+        if (used == 0) {
+          if (ctx->arena_free.empty()) return cudaErrorMemoryAllocation;
+          ctx->pool_chunks[d].push_back(ctx->arena_free.back());
+          ctx->arena_free.pop_back();
+        }
+        const uint64_t c = ctx->pool_chunks[d].back(), m = std::min(kChunk - used, dn - off);
+        e = cudaMemcpyAsync(arena + c * kChunk + used, ctx->pools[d].as<gw_walk_rec>() + off,
+                            m * sizeof(gw_walk_rec), cudaMemcpyDeviceToHost, st);
+        hn += m;
+        off += m;
       }
-      e = pool_async[d] ? cudaFreeAsync(ctx->pools[d].p, st) : cudaFree(ctx->pools[d].p);
+      if (e != cudaSuccess) break;
+      if (dn) ctx->stats.pools_spilled++;
+      if (pool_async[d]) e = cudaFreeAsync(ctx->pools[d].p, st);
+      else sync_free.push_back(ctx->pools[d].p);
       ctx->pools[d].p = nullptr;
       ctx->pools[d].bytes = 0;
       held -= cap[d];
       cap[d] = 0;
       pool_async[d] = 0;
+    }
+    if (!sync_free.empty()) {
+      const cudaError_t e2 = cudaStreamSynchronize(st);
+      for (void* q : sync_free) cudaFree(q);
+      if (e == cudaSuccess) e = e2;
     }
     return e;
   };
@@ -358,16 +391,21 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
     const uint64_t n = ctx->pool_size[b];
     if (n == 0) return ctx->fail(GW_E_STATE, "scheduler chose an empty block (walksum %llu)",
                                  (unsigned long long)walksum);
-    if (!ctx->pool_host[b].empty()) {
+    if (ctx->pool_host_n[b]) {
       // readWalksfromDisk: the pool's host part (its older walks) goes first,
-      // then the walks that arrived on the device since it moved out
-      const uint64_t hn = ctx->pool_host[b].size(), dn = n - hn;
+      // then the walks that arrived on the device since it moved out.  Its
+      // chunks return to the arena at once: whatever reuses them next is a
+      // copy queued on st behind these.
+      const uint64_t hn = ctx->pool_host_n[b], dn = n - hn;
       const uint64_t ncap = std::max<uint64_t>(n, 1024);
       void* np = nullptr;
       e = cudaMallocAsync(&np, ncap * sizeof(gw_walk_rec), st);
       if (e != cudaSuccess) break;
-      // from pageable memory: the records are staged before the call returns
-      e = cudaMemcpyAsync(np, ctx->pool_host[b].data(), hn * sizeof(gw_walk_rec), cudaMemcpyHostToDevice, st);
+      for (uint64_t i = 0; i * kChunk < hn && e == cudaSuccess; ++i) {
+        const uint64_t c = ctx->pool_chunks[b][i], m = std::min(kChunk, hn - i * kChunk);
+        e = cudaMemcpyAsync(static_cast<gw_walk_rec*>(np) + i * kChunk, arena + c * kChunk, m * sizeof(gw_walk_rec),
+                            cudaMemcpyHostToDevice, st);
+      }
       if (e == cudaSuccess && dn)
         e = cudaMemcpyAsync(static_cast<gw_walk_rec*>(np) + hn, ctx->pools[b].p, dn * sizeof(gw_walk_rec),
                             cudaMemcpyDeviceToDevice, st);
@@ -381,7 +419,9 @@ gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p) {
       ctx->pools[b].p = np;
       ctx->pools[b].bytes = ncap * sizeof(gw_walk_rec);
       cap[b] = ncap;
-      std::vector<gw_walk_rec>().swap(ctx->pool_host[b]);
+      for (uint32_t c : ctx->pool_chunks[b]) ctx->arena_free.push_back(c);
+      ctx->pool_chunks[b].clear();
+      ctx->pool_host_n[b] = 0;
       ctx->stats.pools_refilled++;
       if (e != cudaSuccess) break;
     }

@@ -207,7 +207,8 @@ gw_status gw_set_mapped_block_walks(gw_ctx *ctx, uint64_t max_walks);
 /* Device bytes the blocked engine's walk pools may hold (0, the default: no
    limit).  Past it, after a superstep, whole pools move to host memory, the
    pools with the fewest pending walks first (never the fullest, the likely
-   next choice), as WalkManager::writeWalks2Disk spills pool buffers
+   next choice), until the rest hold half the budget, as
+   WalkManager::writeWalks2Disk spills pool buffers
    (walk.hpp:103-112); a block whose pool was moved is brought back, older
    walks first, when it is chosen (readWalksfromDisk, walk.hpp:139-157).  Pool
    order, walks and counts are unchanged; the pool of the block being run may
