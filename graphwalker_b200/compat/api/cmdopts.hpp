@@ -23,6 +23,9 @@
 //                   "auto" (default, per block one walk per 128 bytes of its
 //                   CSR) | a number | 0 (copy every block)
 //                   (gw_set_mapped_block_walks)
+//   gw_pool_budget_mb device MB the blocked engine's walk pools may hold; past
+//                   it pools move to pinned host memory and come back when
+//                   their block runs (default 0: no limit; gw_set_pool_budget)
 //   gw_chunk        walks per device run in replay mode (default 4194304)
 //   gw_device       CUDA device ordinal (default 0)
 //   gw_edge_records "auto" (default): 16-byte edge records when they fit in

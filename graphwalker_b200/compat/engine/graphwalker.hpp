@@ -61,6 +61,9 @@ class graphwalker_engine {
     if (gw_open(&d, &ctx) != GW_OK)
       logstream(LOG_FATAL) << "graphwalker_engine: " << gw_last_error(nullptr) << std::endl;
     m.stop_time("2_findSubGraph");
+    const uint64_t pool_mb = get_option_long("gw_pool_budget_mb", 0);
+    if (gw_set_pool_budget(ctx, pool_mb << 20) != GW_OK)
+      logstream(LOG_FATAL) << "graphwalker_engine: " << gw_last_error(ctx) << std::endl;
     const std::string mapped = get_option_string("gw_mapped_walks", "auto");
     if (gw_set_mapped_block_walks(ctx, mapped == "auto" ? GW_MAPPED_AUTO : strtoull(mapped.c_str(), nullptr, 10)) !=
         GW_OK)

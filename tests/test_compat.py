@@ -108,7 +108,8 @@ def test_compat_streamed_block_loop_counts(cuda_device, mapped, tmp_path):
         r = subprocess.run([str(app), base, str(int(g["blocksize_kb"])), str(tmp_path / "walks.bin"), str(out),
                             str(int(g[f"{tag}_L"])), str(int(g["seed"])), str(nv), "1", "1",
                             "gw_walk_id", "source", "seed", str(int(g["seed"])), "gw_mode", "blocked",
-                            "gw_residency", "stream", "gw_mapped_walks", mapped, "gw_sink", "count"],
+                            "gw_residency", "stream", "gw_mapped_walks", mapped, "gw_sink", "count",
+                            "gw_pool_budget_mb", "1"],
                            cwd=tmp_path, capture_output=True, text=True)
         assert r.returncode == 0, r.stderr[-2000:]
         counts = np.frombuffer(out.read_bytes(), np.uint32, nv, 8)
