@@ -194,6 +194,8 @@ class graphwalker_engine {
     m.add("gpu_ms_partition", st.ms_partition);
     m.add("gpu_ms_copy_wait", st.ms_copy_wait);
     m.add("gpu_blocks_read_in_place", (double)st.mapped_supersteps, INTEGER);
+    m.add("gpu_pools_spilled", (double)st.pools_spilled, INTEGER);
+    m.add("gpu_pools_refilled", (double)st.pools_refilled, INTEGER);
   }
 
   // Runs the walks in chunks that record paths on the device, then calls
