@@ -223,6 +223,29 @@ def test_pool_budget_spills_pools_in_order(cuda_device, oracle, steps, residency
             assert np.array_equal(G.read_counts(), g["jump_counts"])
 
 
+@pytest.mark.parametrize("rule", [0, 1, 3], ids=["jump", "stop", "restart"])
+def test_streamed_in_place_and_spilled_native_rng(cuda_device, oracle, rule):
+    """Both RNG modes through the streamed block loop with every block read in
+    place and the walk pools over a small budget: counts equal the oracle's
+    (which do not depend on the schedule)."""
+    import graphwalker_b200 as gw
+    g = load_golden("rmat13")
+    rp, ci = g["rowptr"], g["colidx"]
+    nv = len(rp) - 1
+    cur = np.arange(nv, dtype=np.uint32)
+    L = 6
+    with _graph(g, gw.STREAM_PINNED) as G:
+        G.set_mapped_block_walks(1 << 40)
+        G.set_pool_budget(32 * 1024)
+        for rng in (0, 1):
+            ref = oracle.run_walks(rp, ci, cur, rule=rule, L=L, seed=11, rng=rng)
+            G.walks_clear()
+            G.add_walks_at(cur)
+            st = G.run(gw.params(rule, gw.SINK_VERTEX_COUNT, L, seed=11, mode=gw.MODE_BLOCKED, rng=rng))
+            assert np.array_equal(G.read_counts(), ref["counts"]), rng
+            assert st.block_loads == 0 and st.pools_spilled > 0
+
+
 def test_device_rmat_matches_oracle(cuda_device, oracle):
     import graphwalker_b200 as gw
     for scale, ef, seed in [(10, 16, 1), (13, 8, 3), (16, 16, 9)]:
