@@ -5,6 +5,7 @@
 //   swapOut (evict fewest walks)       src/engine/graphwalker.hpp:236-251
 //   WalkManager::chooseBlock & co.     src/walks/walk.hpp:204-252
 //   getCurrentWalks / updateWalkNum    src/walks/walk.hpp:114-192
+//   writeWalks2Disk / readWalksfromDisk src/walks/walk.hpp:103-157 (pool budget)
 //
 // Each superstep picks a block with the reference's state-aware policy (with
 // probability `prob` the block holding the lowest-hop walk, otherwise the
@@ -16,7 +17,7 @@
 // the partition's histogram each superstep, through mapped pinned memory, so
 // no small copy of a superstep queues behind a block copy.
 //
-// Streaming differs from findSubGraph in two ways that change neither the
+// Streaming differs from findSubGraph in three ways that change neither the
 // order of blocks nor any walk:
 //  * the row pointer stays in HBM, and a slot holds a block's column slice;
 //  * a chosen block in no slot whose pool is small (ctx->mapped_max_walks,
@@ -26,6 +27,10 @@
 //  * while a block runs, up to kCopyAhead blocks with many pending walks are
 //    copied into slots before their turn, each taking the room of the slot
 //    with the fewest pending walks (swapOut's victim) when it has more.
+//
+// With a pool budget (ctx->pool_budget), walk pools beyond it wait in a
+// pinned host arena, in either residency; a pool is the arena part (older
+// walks) followed by its device part, so pool order is kept.
 #include <algorithm>
 #include <cstring>
 
