@@ -116,6 +116,9 @@ def test_empty_calls(graph):
         out = np.full(nv, 9, np.uint32)
         G.run_pools(p, words, offs, out)
         assert np.all(out == 0)  # the counts of no walks
+        out[:] = 9
+        G.run_pools_wait(G.run_pools_submit(p, words, offs, out))
+        assert np.all(out == 0)
         ids, cnt, st = G.ppr(gw.params(gw.RULE_STOP, gw.SINK_NONE, 20), np.zeros(0, np.uint32),
                              np.zeros(0, np.uint32), k=10)
         assert ids.shape == (0, 10) and st.walks == 0
