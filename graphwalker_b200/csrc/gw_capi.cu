@@ -869,16 +869,12 @@ gw_status gw_run_pools(gw_ctx* ctx, const gw_walk_params* params, const uint64_t
   if (s != GW_OK) return s;
   const uint64_t n = pool_offsets[ctx->nblocks];
   if (n && !words) return ctx->fail(GW_E_INVALID, "words is NULL");
-  // Chunks of the host words are copied on the copy stream while the walk
-  // kernel of the previous chunk runs.  A walk word crosses PCIe faster than
-  // its walk runs, so the chunks start small (the first kernel waits only for
-  // a short copy) and grow by 7/4 each time, which keeps each copy shorter
-  // than the kernel it hides behind.  The chunk kernels alternate between two
-  // compute streams, so a chunk's walks start while the previous kernel's
-  // last walks finish instead of after them (the walks of different chunks
-  // share only the visit counters, updated atomically).
-  std::vector<uint64_t> chunk_lo{0};
-  for (uint64_t m = 1ull << 17; chunk_lo.back() < n; m += m * 3 / 4) chunk_lo.push_back(std::min(n, chunk_lo.back() + m));
+  // Chunks of the host words (gw::chunk_bounds) are copied on the copy stream
+  // while the walk kernel of the previous chunk runs.  The chunk kernels
+  // alternate between two compute streams, so a chunk's walks start while the
+  // previous kernel's last walks finish instead of after them (the walks of
+  // different chunks share only the visit counters, updated atomically).
+  const std::vector<uint64_t> chunk_lo = gw::chunk_bounds(n);
   const uint64_t nchunks = chunk_lo.size() - 1;
   GW_CUDA(ctx, ctx->d_walks.ensure(n * sizeof(gw_walk_rec)), "walk alloc");
   GW_CUDA(ctx, ctx->d_words.ensure(n * 8), "word alloc");

@@ -216,6 +216,12 @@ gw_status status_of(gw_ctx* ctx, uint32_t bits);
 gw_status run_blocked(gw_ctx* ctx, const gw_walk_params* p);
 // Frees the buffers, events and stream of gw_run_pools_submit (gw_pools_async.cu).
 void pipe_release(gw_ctx* ctx);
+// Chunk boundaries (n_chunks + 1 entries) of a host call over n walk words:
+// the walk words cross the host link faster than their walks run, so the
+// chunks start small (the first kernel waits only for a short copy) and grow
+// by 7/4 each time, which keeps each copy shorter than the kernel it hides
+// behind (gw_run_pools, gw_run_pools_submit).
+std::vector<uint64_t> chunk_bounds(uint64_t n);
 }  // namespace gw
 
 #define GW_CUDA(ctx, expr, what)                    \

@@ -34,15 +34,13 @@ cudaError_t pipe_init(gw_ctx* ctx) {
   return e;
 }
 
-// Chunk boundaries of a run of n walks: the same growth as gw_run_pools (a
-// short first copy, then each chunk 7/4 of the last).
+}  // namespace
+
 std::vector<uint64_t> chunk_bounds(uint64_t n) {
   std::vector<uint64_t> lo{0};
   for (uint64_t m = 1ull << 17; lo.back() < n; m += m * 3 / 4) lo.push_back(std::min(n, lo.back() + m));
   return lo;
 }
-
-}  // namespace
 
 void pipe_release(gw_ctx* ctx) {
   auto& P = ctx->pipe;
